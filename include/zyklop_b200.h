@@ -1,0 +1,122 @@
+/*
+ * zyklop_b200 — C ABI of the B200 (sm_100a) Groth16 / BN254 prover library.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a status code
+ * (ZK_OK on success) and never exits the process; zk_last_error() gives the
+ * calling thread's message for the last failure.  Field elements are
+ * 4 x u64 little-endian limbs (the reference's layout); "Montgomery" means
+ * x * 2^256 mod m, as in the reference.
+ *
+ * Each declaration names the reference interface it replaces
+ * (Julienbxl/Zyklop, file:line).
+ */
+#ifndef ZYKLOP_B200_H
+#define ZYKLOP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define ZK_OK 0
+#define ZK_EINVAL 1     /* bad argument or size                        */
+#define ZK_ECUDA 2      /* CUDA runtime error                          */
+#define ZK_ENOMEM 3     /* device or host allocation failed            */
+#define ZK_EIO 4        /* file could not be opened / read             */
+#define ZK_EFORMAT 5    /* malformed zkey / wtns                       */
+#define ZK_EWITNESS 6   /* witness shorter than the circuit needs      */
+#define ZK_ETIMEOUT 7   /* a bounded wait gave up                      */
+#define ZK_EINTERNAL 8  /* unexpected internal failure                 */
+#define ZK_ENOTSUP 9    /* unsupported parameter                       */
+
+typedef struct zk_ctx zk_ctx;
+
+/* Library version string. */
+const char* zk_version(void);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* zk_last_error(void);
+
+/* A context owns one CUDA stream, the device scratch arena and the cached NTT
+ * twiddle tables for one device.  Calls on one context are serialized; use
+ * one context per host thread for concurrency.  Passing ctx = NULL to any
+ * entry point uses a per-device default context (current device).
+ * Replaces the reference's global state (g_ntt_* statics,
+ * include/ntt_bn254.cuh:50-53; implicit device 0 and legacy stream). */
+int zk_ctx_create(int device, zk_ctx** out);
+int zk_ctx_destroy(zk_ctx* ctx);
+/* Synchronize the context's stream. */
+int zk_ctx_sync(zk_ctx* ctx);
+
+/* ---- field primitives (device pointers, n elements of 4 x u64) ----------- */
+#define ZK_FIELD_FP 0
+#define ZK_FIELD_FR 1
+#define ZK_OP_MUL 0     /* Montgomery product                        */
+#define ZK_OP_ADD 1
+#define ZK_OP_SUB 2
+#define ZK_OP_SQR 3
+#define ZK_OP_NEG 4
+#define ZK_OP_INV 5     /* Montgomery inverse (0 -> 0)               */
+#define ZK_OP_ENCODE 6  /* canonical -> Montgomery                   */
+#define ZK_OP_DECODE 7  /* Montgomery -> canonical                   */
+/* out[i] = op(a[i], b[i]); b is ignored by unary ops.  Replaces the
+ * reference's device field functions exercised by its unit tests:
+ * fpMul/fpSqr/fpAdd/fpSub/fpNeg/fpInv (include/fp_bn254.cuh:87-775) and
+ * frMul/frAdd/frSub/frNeg/frInv/frMontEncode/Decode
+ * (include/fr_bn254.cuh:191-321). */
+int zk_field_op(zk_ctx* ctx, int field, int op, uint64_t* d_out, const uint64_t* d_a,
+                const uint64_t* d_b, size_t n);
+
+/* ---- NTT ----------------------------------------------------------------- */
+/* In-place natural-order NTT of 2^log_n Montgomery Fr elements on the device;
+ * inverse != 0 gives the inverse scaled by 1/N.  omega_N = 5^((r-1)/N).
+ * Replaces nttPrepare / ntt / nttDestroy (include/ntt_bn254.cuh:190-281,
+ * 418-464); no prepare call is needed (tables are cached per context). */
+int zk_ntt(zk_ctx* ctx, uint64_t* d_a, uint32_t log_n, int inverse);
+
+/* H evaluations h[j] = (A*B - C)(omega_2n^(2j+1)), canonical, from
+ * d_aw = A.w and d_bw = B.w (Montgomery, 2^log_n each; both are
+ * overwritten).  Replaces computeHPoly (src/groth16.cu:1037-1128). */
+int zk_hpoly(zk_ctx* ctx, uint64_t* d_aw, uint64_t* d_bw, uint32_t log_n, uint64_t* d_h);
+
+/* ---- MSM ------------------------------------------------------------------ */
+/* sum_i k_i * P_i on G1.  d_px, d_py: n x 4 u64 affine Montgomery (SoA,
+ * (0,0) = infinity); d_scalars: n x 4 u64 canonical integers.
+ * h_out: x[4], y[4] affine Montgomery ((0,0) for infinity); *is_inf set if
+ * not NULL.  Blocks until the result is on the host.
+ * Replaces msm_g1 (include/msm_g1.cuh:918-926). */
+int zk_msm_g1(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
+              size_t n, uint64_t* h_out, int* is_inf);
+
+/* Same on G2: d_px, d_py n x 8 u64 ([a0, a1] per coordinate); h_out 16 u64
+ * (x.a0, x.a1, y.a0, y.a1).  Replaces msm_g2_device
+ * (include/msm_g2.cuh:669-854). */
+int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
+              size_t n, uint64_t* h_out, int* is_inf);
+
+/* Pippenger parameters for subsequent MSMs on this context (group 1 or 2):
+ * window bits c (0 = automatic), records per thread k0 / k1, buckets per
+ * thread in the bucket reduction.  Replaces the reference's compile-time
+ * MSM_G1_C_BITS / C_BITS and ZK_G1_* / ZK_G2_* environment knobs
+ * (include/msm_g1.cuh:45-117, include/msm_g2.cuh:39-116). */
+int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk);
+
+/* Device scratch bytes an MSM of n points needs under the current config. */
+int zk_msm_scratch_bytes(zk_ctx* ctx, int group, size_t n, size_t* bytes);
+
+/* ---- setup helpers --------------------------------------------------------- */
+/* d_px[i], d_py[i] = k_i * G (affine Montgomery) for the standard generator of
+ * G1 (group 1; 4 u64 per coordinate) or G2 (group 2; 8 u64), k_i canonical
+ * (n x 4 u64).  No reference counterpart: the reference's CRS points come
+ * from snarkjs; this builds seeded synthetic CRS points and MSM bases. */
+int zk_mul_generator(zk_ctx* ctx, int group, const uint64_t* d_scalars, size_t n, uint64_t* d_px,
+                     uint64_t* d_py);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZYKLOP_B200_H */

@@ -1,0 +1,72 @@
+"""ctypes binding of libzyklop_b200.so (signatures of include/zyklop_b200.h)."""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libzyklop_b200.so")
+
+_lib = None
+
+u64p = ctypes.POINTER(ctypes.c_uint64)
+u8p = ctypes.POINTER(ctypes.c_uint8)
+c_int_p = ctypes.POINTER(ctypes.c_int)
+sz = ctypes.c_size_t
+
+
+class ZkError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"zyklop_b200 error {code}: {msg}")
+        self.code = code
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "zk_version": (ctypes.c_char_p, []),
+    "zk_last_error": (ctypes.c_char_p, []),
+    "zk_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "zk_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "zk_ctx_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "zk_field_op": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p, sz]),
+    "zk_ntt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int]),
+    "zk_hpoly": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                ctypes.c_void_p]),
+    "zk_msm_g1": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                 sz, u64p, c_int_p]),
+    "zk_msm_g2": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                 sz, u64p, c_int_p]),
+    "zk_msm_set_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int]),
+    "zk_msm_scratch_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, sz,
+                                            ctypes.POINTER(ctypes.c_size_t)]),
+    "zk_mul_generator": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, sz,
+                                        ctypes.c_void_p, ctypes.c_void_p]),
+}
+
+
+def lib():
+    """Load the library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make -C zyklop_b200/csrc` "
+            "(or __graft_entry__.build()); there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != 0:
+        raise ZkError(rc, lib().zk_last_error().decode())
+    return rc
+
+
+def version():
+    return lib().zk_version().decode()

@@ -1,0 +1,244 @@
+// C ABI entry points for contexts and primitives (include/zyklop_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "context.hpp"
+#include "field.cuh"
+
+namespace zk {
+const char* last_error();
+void mul_generator(int group, const uint64_t* scalars, size_t n, uint64_t* px, uint64_t* py,
+                   cudaStream_t st);
+
+namespace {
+
+std::mutex g_default_mu;
+std::vector<zk_ctx*> g_defaults;
+
+template <class C>
+__global__ void k_field_op(int op, fe<C>* __restrict__ out, const fe<C>* __restrict__ a,
+                           const fe<C>* __restrict__ b, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const fe<C> x = fe_load<C>(a, i);
+  fe<C> r;
+  switch (op) {
+    case ZK_OP_MUL: r = x * fe_load<C>(b, i); break;
+    case ZK_OP_ADD: r = x + fe_load<C>(b, i); break;
+    case ZK_OP_SUB: r = x - fe_load<C>(b, i); break;
+    case ZK_OP_SQR: r = fe_sqr(x); break;
+    case ZK_OP_NEG: r = fe_neg(x); break;
+    case ZK_OP_INV: r = fe_inv(x); break;
+    case ZK_OP_ENCODE: r = fe_to_mont(x); break;
+    default: r = fe_from_mont(x); break;
+  }
+  fe_store(out, i, r);
+}
+
+}  // namespace
+
+zk_ctx* default_ctx() {
+  int dev = 0;
+  ZK_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(g_default_mu);
+  if ((int)g_defaults.size() <= dev) g_defaults.resize(dev + 1, nullptr);
+  if (!g_defaults[dev]) {
+    zk_ctx* c = new zk_ctx();
+    c->device = dev;
+    c->is_default = true;
+    ZK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    g_defaults[dev] = c;
+  }
+  return g_defaults[dev];
+}
+
+void use_device(zk_ctx* ctx) { ZK_CUDA(cudaSetDevice(ctx->device)); }
+
+}  // namespace zk
+
+using namespace zk;
+
+#define ZK_API_BEGIN try {
+#define ZK_API_END                                       \
+  }                                                      \
+  catch (const zk::Error& e) {                           \
+    zk::set_last_error(e.code, e.what());                \
+    return e.code;                                       \
+  }                                                      \
+  catch (const std::bad_alloc&) {                        \
+    zk::set_last_error(ZK_ENOMEM, "host allocation failed"); \
+    return ZK_ENOMEM;                                    \
+  }                                                      \
+  catch (const std::exception& e) {                      \
+    zk::set_last_error(ZK_EINTERNAL, e.what());          \
+    return ZK_EINTERNAL;                                 \
+  }                                                      \
+  zk::set_last_error(ZK_OK, "");                         \
+  return ZK_OK;
+
+static zk_ctx* resolve(zk_ctx* ctx) {
+  if (!ctx) return default_ctx();
+  use_device(ctx);
+  return ctx;
+}
+
+extern "C" {
+
+const char* zk_version(void) { return "zyklop_b200 0.1.0 (sm_100a)"; }
+
+const char* zk_last_error(void) { return zk::last_error(); }
+
+int zk_ctx_create(int device, zk_ctx** out) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(out, ZK_EINVAL, "zk_ctx_create: out is NULL");
+  *out = nullptr;
+  int count = 0;
+  ZK_CUDA(cudaGetDeviceCount(&count));
+  ZK_REQUIRE(device >= 0 && device < count, ZK_EINVAL, "zk_ctx_create: no such device");
+  ZK_CUDA(cudaSetDevice(device));
+  zk_ctx* c = new zk_ctx();
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    throw_cuda(e, "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+  }
+  *out = c;
+  ZK_API_END
+}
+
+int zk_ctx_destroy(zk_ctx* ctx) {
+  ZK_API_BEGIN
+  if (!ctx || ctx->is_default) return ZK_OK;
+  use_device(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  ZK_API_END
+}
+
+int zk_ctx_sync(zk_ctx* ctx) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  ZK_API_END
+}
+
+int zk_field_op(zk_ctx* ctx, int field, int op, uint64_t* d_out, const uint64_t* d_a,
+                const uint64_t* d_b, size_t n) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_REQUIRE(field == ZK_FIELD_FP || field == ZK_FIELD_FR, ZK_EINVAL, "zk_field_op: bad field");
+  ZK_REQUIRE(op >= 0 && op <= ZK_OP_DECODE, ZK_EINVAL, "zk_field_op: bad op");
+  ZK_REQUIRE(n == 0 || (d_out && d_a), ZK_EINVAL, "zk_field_op: NULL buffer");
+  const bool binary = op == ZK_OP_MUL || op == ZK_OP_ADD || op == ZK_OP_SUB;
+  ZK_REQUIRE(!binary || n == 0 || d_b, ZK_EINVAL, "zk_field_op: binary op needs b");
+  if (n) {
+    const unsigned g = (unsigned)((n + 255) / 256);
+    if (field == ZK_FIELD_FP)
+      k_field_op<FpCfg><<<g, 256, 0, ctx->stream>>>(op, reinterpret_cast<fp_t*>(d_out),
+                                                    reinterpret_cast<const fp_t*>(d_a),
+                                                    reinterpret_cast<const fp_t*>(d_b), n);
+    else
+      k_field_op<FrCfg><<<g, 256, 0, ctx->stream>>>(op, reinterpret_cast<fr_t*>(d_out),
+                                                    reinterpret_cast<const fr_t*>(d_a),
+                                                    reinterpret_cast<const fr_t*>(d_b), n);
+    ZK_CHECK_LAUNCH();
+  }
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  ZK_API_END
+}
+
+int zk_ntt(zk_ctx* ctx, uint64_t* d_a, uint32_t log_n, int inverse) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_REQUIRE(d_a, ZK_EINVAL, "zk_ntt: NULL buffer");
+  ZK_REQUIRE(log_n <= (uint32_t)kMaxLogN, ZK_EINVAL, "zk_ntt: log_n > 27");
+  ctx->ntt_scratch.ensure((size_t)32 << log_n);
+  ntt_inplace(ctx->ntt, d_a, (int)log_n, inverse != 0, ctx->ntt_scratch.ptr, ctx->stream);
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  ZK_API_END
+}
+
+int zk_hpoly(zk_ctx* ctx, uint64_t* d_aw, uint64_t* d_bw, uint32_t log_n, uint64_t* d_h) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_REQUIRE(d_aw && d_bw && d_h, ZK_EINVAL, "zk_hpoly: NULL buffer");
+  ZK_REQUIRE(log_n >= 1 && log_n < (uint32_t)kMaxLogN, ZK_EINVAL, "zk_hpoly: log_n out of range");
+  ctx->ntt_scratch.ensure((size_t)32 << log_n);
+  hpoly(ctx->ntt, d_aw, d_bw, ctx->ntt_scratch.as<uint64_t>(), (int)log_n, d_h, ctx->stream);
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  ZK_API_END
+}
+
+int zk_msm_g1(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
+              size_t n, uint64_t* h_out, int* is_inf) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_REQUIRE(h_out, ZK_EINVAL, "zk_msm_g1: NULL output");
+  ZK_REQUIRE(n == 0 || (d_px && d_py && d_scalars), ZK_EINVAL, "zk_msm_g1: NULL input");
+  const bool inf = msm_g1_run(d_px, d_py, d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[0],
+                              ctx->stream, h_out);
+  if (is_inf) *is_inf = inf ? 1 : 0;
+  ZK_API_END
+}
+
+int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
+              size_t n, uint64_t* h_out, int* is_inf) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_REQUIRE(h_out, ZK_EINVAL, "zk_msm_g2: NULL output");
+  ZK_REQUIRE(n == 0 || (d_px && d_py && d_scalars), ZK_EINVAL, "zk_msm_g2: NULL input");
+  const bool inf = msm_g2_run(d_px, d_py, d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[1],
+                              ctx->stream, h_out);
+  if (is_inf) *is_inf = inf ? 1 : 0;
+  ZK_API_END
+}
+
+int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_msm_set_config: group must be 1 or 2");
+  ZK_REQUIRE(c == 0 || (c >= 4 && c <= 21), ZK_EINVAL, "zk_msm_set_config: c must be 0 or 4..21");
+  ZK_REQUIRE(k0 >= 1 && k0 <= 4096 && k1 >= 2 && k1 <= 4096, ZK_EINVAL,
+             "zk_msm_set_config: k0 in 1..4096, k1 in 2..4096");
+  ZK_REQUIRE(chunk >= 1 && chunk <= 4096, ZK_EINVAL, "zk_msm_set_config: chunk in 1..4096");
+  MsmConfig& m = ctx->msm_cfg[group - 1];
+  m.c = c;
+  m.k0 = k0;
+  m.k1 = k1;
+  m.chunk = chunk;
+  ZK_API_END
+}
+
+int zk_msm_scratch_bytes(zk_ctx* ctx, int group, size_t n, size_t* bytes) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  ZK_REQUIRE(bytes, ZK_EINVAL, "zk_msm_scratch_bytes: NULL output");
+  ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_msm_scratch_bytes: group must be 1 or 2");
+  *bytes = msm_scratch_bytes(n, group == 2, ctx->msm_cfg[group - 1]);
+  ZK_API_END
+}
+
+int zk_mul_generator(zk_ctx* ctx, int group, const uint64_t* d_scalars, size_t n, uint64_t* d_px,
+                     uint64_t* d_py) {
+  ZK_API_BEGIN
+  ctx = resolve(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_mul_generator: group must be 1 or 2");
+  ZK_REQUIRE(n == 0 || (d_scalars && d_px && d_py), ZK_EINVAL, "zk_mul_generator: NULL buffer");
+  mul_generator(group, d_scalars, n, d_px, d_py, ctx->stream);
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  ZK_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,671 @@
+// Pippenger MSM on G1 / G2 for sm_100a.  See msm.hpp for the pipeline; the
+// reference counterpart is include/msm_g1.cuh:271-926 and
+// include/msm_g2.cuh:256-880.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "curve.cuh"
+#include "host_field.hpp"
+#include "msm.hpp"
+
+namespace zk {
+namespace {
+
+constexpr uint32_t kInvalid = 0xffffffffu;
+constexpr uint32_t kNeg = 0x80000000u;
+constexpr int kScanTile = 4096;   // entries per scan block (1024 threads x 4)
+
+// ------------------------------------------------------------------ shape
+struct Shape {
+  size_t n;
+  int c, W;
+  uint32_t B;            // buckets per window (2^(c-1))
+  size_t entries;        // W*B + 1 scan entries (last = total)
+  size_t records;        // W*n upper bound on sorted records
+  int k0, k1, chunk;
+  int levels;            // segmented-reduction levels (>= 1)
+  size_t lvl_records[24];
+  size_t lvl_blocks[24];
+  size_t J;              // bucket-reduction chunks per window
+};
+
+Shape make_shape(size_t n, bool g2, const MsmConfig& cfg) {
+  const int seg_t = g2 ? 64 : 128;
+  Shape s{};
+  s.n = n;
+  s.c = cfg.c > 0 ? cfg.c : msm_default_c(n, g2);
+  s.W = 256 / s.c + 1;  // top window holds < c bits, so no carry leaves it
+  s.B = 1u << (s.c - 1);
+  s.entries = (size_t)s.W * s.B + 1;
+  s.records = std::max<size_t>((size_t)s.W * n, 1);
+  s.k0 = cfg.k0;
+  s.k1 = cfg.k1;
+  s.chunk = cfg.chunk;
+  s.J = (s.B + s.chunk - 1) / s.chunk;
+  size_t rec = s.records;
+  int per_thread = s.k0;
+  s.levels = 0;
+  while (true) {
+    size_t per_block = (size_t)seg_t * per_thread;
+    size_t blocks = (rec + per_block - 1) / per_block;
+    s.lvl_records[s.levels] = rec;
+    s.lvl_blocks[s.levels] = blocks;
+    s.levels++;
+    if (blocks <= 1 || s.levels == 24) break;
+    rec = 2 * blocks;
+    per_thread = s.k1;
+  }
+  return s;
+}
+
+template <class F>
+struct Layout {
+  uint32_t* counts;   // entries (exclusive offsets after the scan)
+  uint32_t* cursor;   // entries
+  uint32_t* tiles;    // scan tile sums
+  uint32_t* skey;     // records
+  uint32_t* sval;     // records
+  xyzz<F>* buckets;   // W*B
+  uint32_t* pkey[2];  // ping-pong partial records
+  xyzz<F>* ppt[2];
+  xyzz<F>* contrib;   // W*J
+  xyzz<F>* windows;   // W
+  size_t bytes;
+};
+
+template <class F>
+Layout<F> carve(void* base, const Shape& s) {
+  Layout<F> L{};
+  Carver cv(base);
+  L.counts = cv.take<uint32_t>(s.entries);
+  L.cursor = cv.take<uint32_t>(s.entries);
+  L.tiles = cv.take<uint32_t>((s.entries + kScanTile - 1) / kScanTile + 1);
+  L.skey = cv.take<uint32_t>(s.records);
+  L.sval = cv.take<uint32_t>(s.records);
+  L.buckets = cv.take<xyzz<F>>((size_t)s.W * s.B);
+  size_t pmax[2] = {1, 1};
+  for (int l = 1; l < s.levels; l++) pmax[l & 1] = std::max(pmax[l & 1], s.lvl_records[l]);
+  for (int i = 0; i < 2; i++) {
+    L.pkey[i] = cv.take<uint32_t>(pmax[i]);
+    L.ppt[i] = cv.take<xyzz<F>>(pmax[i]);
+  }
+  L.contrib = cv.take<xyzz<F>>((size_t)s.W * s.J);
+  L.windows = cv.take<xyzz<F>>((size_t)s.W);
+  L.bytes = cv.off + 256;
+  return L;
+}
+
+// --------------------------------------------------------------- digits
+__device__ __forceinline__ void load_scalar(const uint64_t* sc, size_t i, uint32_t s[8]) {
+  const uint4* p = reinterpret_cast<const uint4*>(sc) + 2 * i;
+  uint4 a = __ldg(p), b = __ldg(p + 1);
+  s[0] = a.x; s[1] = a.y; s[2] = a.z; s[3] = a.w;
+  s[4] = b.x; s[5] = b.y; s[6] = b.z; s[7] = b.w;
+}
+
+// Pops the next c-bit window off a 256-bit scalar (s >>= c) and returns it.
+__device__ __forceinline__ uint32_t pop_window(uint32_t s[8], int c) {
+  const uint32_t v = s[0] & ((1u << c) - 1u);
+#pragma unroll
+  for (int i = 0; i < 7; i++) s[i] = __funnelshift_r(s[i], s[i + 1], c);
+  s[7] >>= c;
+  return v;
+}
+
+// Signed-digit recoding, digit in [-2^(c-1), 2^(c-1)]: the same digit set as
+// the reference's g1_extractAllSigned (include/msm_g1.cuh:271-329).
+// Returns the (window, bucket) key or kInvalid for a zero digit.
+__device__ __forceinline__ uint32_t next_digit(uint32_t s[8], int c, uint32_t B, int w,
+                                               uint32_t& carry, bool& neg) {
+  uint32_t raw = pop_window(s, c) + carry;
+  uint32_t mag;
+  if (raw > B) {
+    mag = (1u << c) - raw;
+    carry = 1;
+    neg = true;
+  } else {
+    mag = raw;
+    carry = 0;
+    neg = false;
+  }
+  return mag ? (uint32_t)w * B + (mag - 1) : kInvalid;
+}
+
+__global__ void k_msm_hist(const uint64_t* __restrict__ sc, size_t n, int c, int W, uint32_t B,
+                           uint32_t* __restrict__ counts) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i < n;
+  uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (active) load_scalar(sc, i, s);
+  const int lane = threadIdx.x & 31;
+  uint32_t carry = 0;
+  for (int w = 0; w < W; w++) {
+    bool neg;
+    uint32_t key = next_digit(s, c, B, w, carry, neg);
+    if (!active) key = kInvalid;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (key != kInvalid && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
+  }
+}
+
+__global__ void k_msm_scatter(const uint64_t* __restrict__ sc, size_t n, int c, int W, uint32_t B,
+                              uint32_t* __restrict__ cursor, uint32_t* __restrict__ skey,
+                              uint32_t* __restrict__ sval) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i < n;
+  uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (active) load_scalar(sc, i, s);
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  uint32_t carry = 0;
+  for (int w = 0; w < W; w++) {
+    bool neg;
+    uint32_t key = next_digit(s, c, B, w, carry, neg);
+    if (!active) key = kInvalid;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (key != kInvalid && lane == leader) base = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (key != kInvalid) {
+      const uint32_t pos = base + __popc(peers & lt);
+      skey[pos] = key;
+      sval[pos] = (uint32_t)i | (neg ? kNeg : 0u);
+    }
+  }
+}
+
+// ----------------------------------------------------------------- scan
+// Exclusive scan of `entries` u32 counts in three steps: per-tile scan,
+// scan of tile sums, add tile bases (and copy into the scatter cursor).
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sm_warp, uint32_t& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm_warp[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t t = lane < nw ? sm_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < nw) sm_warp[lane] = t;
+  }
+  __syncthreads();
+  const uint32_t warp_base = wid ? sm_warp[wid - 1] : 0;
+  total = sm_warp[nw - 1];
+  __syncthreads();
+  return warp_base + x - v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(uint32_t* __restrict__ a, size_t n,
+                                                     uint32_t* __restrict__ tiles) {
+  __shared__ uint32_t sw[32];
+  const size_t base = (size_t)blockIdx.x * kScanTile + threadIdx.x * 4;
+  uint32_t v[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) v[j] = base + j < n ? a[base + j] : 0;
+  const uint32_t sum = v[0] + v[1] + v[2] + v[3];
+  uint32_t total;
+  uint32_t run = block_excl_scan(sum, sw, total);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (base + j < n) a[base + j] = run;
+    run += v[j];
+  }
+  if (threadIdx.x == 0) tiles[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(uint32_t* __restrict__ tiles, int nt) {
+  __shared__ uint32_t sw[32];
+  // up to 4096 tiles: 4 per thread
+  uint32_t v[4];
+  const int base = threadIdx.x * 4;
+#pragma unroll
+  for (int j = 0; j < 4; j++) v[j] = base + j < nt ? tiles[base + j] : 0;
+  uint32_t total;
+  uint32_t run = block_excl_scan(v[0] + v[1] + v[2] + v[3], sw, total);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (base + j < nt) tiles[base + j] = run;
+    run += v[j];
+  }
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ a, uint32_t* __restrict__ cursor, size_t n,
+                           const uint32_t* __restrict__ tiles) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const uint32_t v = a[i] + tiles[i / kScanTile];
+    a[i] = v;
+    cursor[i] = v;
+  }
+}
+
+// ------------------------------------------------- segmented reduction
+// Node of the block-level segmented reduction: the partial sums of the first
+// and last key-segments of a contiguous record range (one sum if the range
+// holds a single segment).  Complete segments are written to their bucket as
+// soon as they are known to be complete.  Nodes live in shared memory (one
+// per thread) so the serial phase only keeps its running sum in registers.
+template <class F>
+struct __align__(16) SegNode {
+  xyzz<F> f, l;
+  uint32_t fk, lk;  // first / last key (fk == kInvalid: empty node)
+  uint32_t single;
+  uint32_t pad_;
+};
+
+template <class F>
+constexpr int seg_threads() { return sizeof(F) == 32 ? 128 : 64; }
+
+template <class F>
+__device__ __forceinline__ void seg_merge(SegNode<F>& a, const SegNode<F>& b, xyzz<F>* buckets) {
+  if (b.fk == kInvalid) return;
+  if (a.fk == kInvalid) {
+    a = b;
+    return;
+  }
+  if (a.lk == b.fk) {
+    const xyzz<F> j = xyzz_add(a.single ? a.f : a.l, b.f);
+    if (a.single && b.single) {
+      a.f = j;
+    } else if (a.single) {
+      a.f = j;
+      a.l = b.l;
+      a.single = 0;
+    } else if (b.single) {
+      a.l = j;
+    } else {
+      st_pod(&buckets[a.lk], j);
+      a.l = b.l;
+    }
+    a.lk = b.lk;
+  } else {
+    if (!a.single) st_pod(&buckets[a.lk], a.l);
+    if (!b.single) st_pod(&buckets[b.fk], b.f);
+    a.l = b.single ? b.f : b.l;
+    a.lk = b.lk;
+    a.single = 0;
+  }
+}
+
+// Closes the running segment `cur` (sum `acc`) of the thread's node.
+template <class F>
+__device__ __forceinline__ void seg_close(SegNode<F>& nd, const xyzz<F>& acc, uint32_t cur,
+                                          xyzz<F>* buckets) {
+  if (cur == kInvalid) return;
+  if (nd.fk == kInvalid) {
+    nd.fk = cur;
+    nd.f = acc;
+    nd.lk = cur;
+    nd.single = 1;
+  } else {
+    // the previous last segment is now a middle segment: complete
+    if (!nd.single) st_pod(&buckets[nd.lk], nd.l);
+    nd.lk = cur;
+    nd.l = acc;
+    nd.single = 0;
+  }
+}
+
+// Block tree over the per-thread nodes, then emit the block's boundary
+// segments: complete ones go to their buckets, the others become partial
+// records 2*block and 2*block+1 for the next level.
+template <class F>
+__device__ __forceinline__ void seg_block_finish(SegNode<F>* sm, uint32_t key_before,
+                                                 uint32_t key_after, xyzz<F>* buckets,
+                                                 uint32_t* okey, xyzz<F>* opt) {
+  constexpr int T = seg_threads<F>();
+  const int t = threadIdx.x;
+  __syncthreads();
+  for (int s = 1; s < T; s <<= 1) {
+    if ((t & (2 * s - 1)) == 0) seg_merge(sm[t], sm[t + s], buckets);
+    __syncthreads();
+  }
+  if (t != 0) return;
+  const SegNode<F>& r = sm[0];
+  uint32_t hk = kInvalid, tk = kInvalid;
+  const size_t b = blockIdx.x;
+  if (r.fk != kInvalid) {
+    const bool head = key_before == r.fk;
+    if (r.single) {
+      const bool tail = key_after == r.fk;
+      if (!head && !tail) {
+        st_pod(&buckets[r.fk], r.f);
+      } else {
+        hk = r.fk;
+        st_pod(&opt[2 * b], r.f);
+        if (tail) {
+          tk = r.fk;
+          st_pod(&opt[2 * b + 1], xyzz_inf<F>());
+        }
+      }
+    } else {
+      if (head) {
+        hk = r.fk;
+        st_pod(&opt[2 * b], r.f);
+      } else {
+        st_pod(&buckets[r.fk], r.f);
+      }
+      if (key_after == r.lk) {
+        tk = r.lk;
+        st_pod(&opt[2 * b + 1], r.l);
+      } else {
+        st_pod(&buckets[r.lk], r.l);
+      }
+    }
+  }
+  if (okey) {
+    okey[2 * b] = hk;
+    okey[2 * b + 1] = tk;
+  }
+}
+
+// Level 0: records are (bucket key, point index | sign) in bucket order.
+template <class F>
+__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
+    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
+    const uint32_t* __restrict__ total_p, const F* __restrict__ px, const F* __restrict__ py, int K,
+    xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
+  constexpr int T = seg_threads<F>();
+  __shared__ SegNode<F> sm[T];
+  SegNode<F>& nd = sm[threadIdx.x];
+  nd.fk = nd.lk = kInvalid;
+  nd.single = 1;
+  const size_t total = *total_p;
+  const size_t bstart = (size_t)blockIdx.x * T * K;
+  const size_t bend = min(bstart + (size_t)T * K, total);
+  uint32_t key_before = kInvalid, key_after = kInvalid;
+  if (bstart < total) {
+    key_before = bstart ? skey[bstart - 1] : kInvalid;
+    key_after = bend < total ? skey[bend] : kInvalid;
+    const size_t s = bstart + (size_t)threadIdx.x * K;
+    const size_t e = min(s + K, bend);
+    xyzz<F> acc = xyzz_inf<F>();
+    uint32_t cur = kInvalid;
+    for (size_t p = s; p < e; p++) {
+      const uint32_t key = skey[p];
+      if (key != cur) {
+        seg_close(nd, acc, cur, buckets);
+        cur = key;
+        acc = xyzz_inf<F>();
+      }
+      const uint32_t v = sval[p];
+      const uint32_t idx = v & ~kNeg;
+      const F x = ld_pod(px + idx);
+      F y = ld_pod(py + idx);
+      if (!(fe_is_zero(x) && fe_is_zero(y))) {
+        if (v & kNeg) y = fe_neg(y);
+        acc = xyzz_madd(acc, x, y);
+      }
+    }
+    seg_close(nd, acc, cur, buckets);
+  }
+  seg_block_finish(sm, key_before, key_after, buckets, okey, opt);
+}
+
+// Levels >= 1: records are (bucket key, XYZZ partial sum); kInvalid keys
+// carry nothing and only ever separate different keys.
+template <class F>
+__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accumN(
+    const uint32_t* __restrict__ ikey, const xyzz<F>* __restrict__ ipt, size_t m, int K,
+    xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
+  constexpr int T = seg_threads<F>();
+  __shared__ SegNode<F> sm[T];
+  SegNode<F>& nd = sm[threadIdx.x];
+  nd.fk = nd.lk = kInvalid;
+  nd.single = 1;
+  const size_t bstart = (size_t)blockIdx.x * T * K;
+  const size_t bend = min(bstart + (size_t)T * K, m);
+  uint32_t key_before = kInvalid, key_after = kInvalid;
+  if (bstart < m) {
+    key_before = bstart ? ikey[bstart - 1] : kInvalid;
+    key_after = bend < m ? ikey[bend] : kInvalid;
+    const size_t s = bstart + (size_t)threadIdx.x * K;
+    const size_t e = min(s + K, bend);
+    xyzz<F> acc = xyzz_inf<F>();
+    uint32_t cur = kInvalid;
+    for (size_t p = s; p < e; p++) {
+      const uint32_t key = ikey[p];
+      if (key == kInvalid) continue;
+      if (key != cur) {
+        seg_close(nd, acc, cur, buckets);
+        cur = key;
+        acc = xyzz_inf<F>();
+      }
+      acc = xyzz_add(acc, ld_pod(ipt + p));
+    }
+    seg_close(nd, acc, cur, buckets);
+  }
+  seg_block_finish(sm, key_before, key_after, buckets, okey, opt);
+}
+
+// ------------------------------------------------------ bucket reduction
+template <class F>
+__device__ __forceinline__ xyzz<F> xyzz_mul_small(const xyzz<F>& p, uint32_t k) {
+  xyzz<F> r = xyzz_inf<F>();
+  if (k == 0) return r;
+  const int top = 31 - __clz(k);
+  r = p;
+  for (int i = top - 1; i >= 0; i--) {
+    r = xyzz_dbl(r);
+    if ((k >> i) & 1) r = xyzz_add(r, p);
+  }
+  return r;
+}
+
+// thread per (window, chunk): sum_{b in chunk} (b+1) S_b
+template <class F>
+__global__ void __launch_bounds__(128) k_msm_bucket_reduce(const xyzz<F>* __restrict__ buckets,
+                                                           int c, int W, uint32_t B, int chunk,
+                                                           size_t J, xyzz<F>* __restrict__ contrib) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)W * J) return;
+  const int w = (int)(t / J);
+  const uint32_t j = (uint32_t)(t % J);
+  const int nbits = 256 - w * c;
+  const uint32_t Bw = nbits >= c ? B : (nbits <= 0 ? 1u : (1u << nbits));
+  const uint32_t lo = j * chunk;
+  xyzz<F> out = xyzz_inf<F>();
+  if (lo < Bw) {
+    const uint32_t hi = min(lo + (uint32_t)chunk, Bw);
+    const xyzz<F>* bw = buckets + (size_t)w * B;
+    xyzz<F> run = xyzz_inf<F>(), acc = xyzz_inf<F>();
+    for (uint32_t b = hi; b-- > lo;) {
+      run = xyzz_add(run, ld_pod(bw + b));
+      acc = xyzz_add(acc, run);
+    }
+    // buckets lo..hi-1 hold digits lo+1..hi: add lo * run for the offset
+    out = xyzz_add(acc, xyzz_mul_small(run, lo));
+  }
+  st_pod(&contrib[t], out);
+}
+
+// block per window: tree-sum of its chunk contributions
+template <class F>
+__global__ void __launch_bounds__(128) k_msm_window_reduce(const xyzz<F>* __restrict__ contrib,
+                                                           size_t J, xyzz<F>* __restrict__ windows) {
+  __shared__ xyzz<F> sm[128];
+  const int w = blockIdx.x, t = threadIdx.x;
+  xyzz<F> acc = xyzz_inf<F>();
+  for (size_t j = t; j < J; j += blockDim.x) acc = xyzz_add(acc, ld_pod(contrib + (size_t)w * J + j));
+  sm[t] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (t < s) sm[t] = xyzz_add(sm[t], sm[t + s]);
+    __syncthreads();
+  }
+  if (t == 0) st_pod(&windows[w], sm[0]);
+}
+
+// --------------------------------------------------------------- driver
+template <class F>
+int msm_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                void* scratch, size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t st,
+                const void** d_windows, int* c_out) {
+  constexpr bool g2 = sizeof(F) == 64;
+  ZK_REQUIRE(n < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
+  const Shape s = make_shape(n, g2, cfg);
+  ZK_REQUIRE(s.c >= 4 && s.c <= 24, ZK_EINVAL, "msm: window size must be in [4, 24]");
+  ZK_REQUIRE(s.records < (size_t(1) << 32) - 1, ZK_EINVAL, "msm: too many (point, window) records");
+  Layout<F> L = carve<F>(scratch, s);
+  ZK_REQUIRE(L.bytes <= scratch_bytes, ZK_EINVAL, "msm: scratch buffer too small");
+
+  ZK_CUDA(cudaMemsetAsync(L.counts, 0, s.entries * sizeof(uint32_t), st));
+  ZK_CUDA(cudaMemsetAsync(L.buckets, 0, (size_t)s.W * s.B * sizeof(xyzz<F>), st));
+  if (n) {
+    const int th = 256;
+    const unsigned g = (unsigned)((n + th - 1) / th);
+    k_msm_hist<<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
+    ZK_CHECK_LAUNCH();
+  }
+  const int nt = (int)((s.entries + kScanTile - 1) / kScanTile);
+  ZK_REQUIRE(nt <= 4096, ZK_EINVAL, "msm: bucket table too large for the scan");
+  k_scan_tiles<<<nt, 1024, 0, st>>>(L.counts, s.entries, L.tiles);
+  k_scan_top<<<1, 1024, 0, st>>>(L.tiles, nt);
+  k_scan_add<<<(unsigned)((s.entries + 255) / 256), 256, 0, st>>>(L.counts, L.cursor, s.entries, L.tiles);
+  ZK_CHECK_LAUNCH();
+  if (n) {
+    const int th = 256;
+    const unsigned g = (unsigned)((n + th - 1) / th);
+    k_msm_scatter<<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
+    ZK_CHECK_LAUNCH();
+  }
+  const uint32_t* total_p = L.counts + (s.entries - 1);
+  const F* fx = reinterpret_cast<const F*>(px);
+  const F* fy = reinterpret_cast<const F*>(py);
+  // level 0
+  {
+    uint32_t* ok = s.levels > 1 ? L.pkey[1] : nullptr;
+    k_msm_accum0<F><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
+        L.skey, L.sval, total_p, fx, fy, s.k0, L.buckets, ok, L.ppt[1]);
+    ZK_CHECK_LAUNCH();
+  }
+  for (int l = 1; l < s.levels; l++) {
+    const int in = l & 1, out = in ^ 1;
+    uint32_t* ok = (l + 1 < s.levels) ? L.pkey[out] : nullptr;
+    k_msm_accumN<F><<<(unsigned)s.lvl_blocks[l], seg_threads<F>(), 0, st>>>(
+        L.pkey[in], L.ppt[in], s.lvl_records[l], s.k1, L.buckets, ok, L.ppt[out]);
+    ZK_CHECK_LAUNCH();
+  }
+  {
+    const size_t tot = (size_t)s.W * s.J;
+    k_msm_bucket_reduce<F><<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(L.buckets, s.c, s.W, s.B,
+                                                                           s.chunk, s.J, L.contrib);
+    k_msm_window_reduce<F><<<s.W, 128, 0, st>>>(L.contrib, s.J, L.windows);
+    ZK_CHECK_LAUNCH();
+  }
+  *d_windows = L.windows;
+  *c_out = s.c;
+  return s.W;
+}
+
+}  // namespace
+
+int msm_default_c(size_t n, bool g2) {
+  // ~N / 2^c records per bucket; tuned by measurement (see bench sweeps)
+  int lg = 0;
+  while ((size_t(1) << lg) < n) lg++;
+  int c = lg - (g2 ? 4 : 4);
+  if (c < 4) c = 4;
+  if (c > 18) c = 18;
+  return c;
+}
+
+size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg) {
+  const Shape s = make_shape(n, g2, cfg);
+  if (g2) return carve<fp2_t>(nullptr, s).bytes;
+  return carve<fp_t>(nullptr, s).bytes;
+}
+
+int msm_g1_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                   void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st,
+                   const void** d_windows, int* c_out) {
+  return msm_enqueue<fp_t>(px, py, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
+}
+int msm_g2_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                   void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st,
+                   const void** d_windows, int* c_out) {
+  return msm_enqueue<fp2_t>(px, py, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
+}
+
+namespace {
+host::Fp fp_from_words(const uint32_t* w) {
+  host::Fp r;
+  memcpy(r.v, w, 32);
+  return r;
+}
+}  // namespace
+
+bool msm_g1_combine(const void* h_windows, int W, int c, uint64_t out[8]) {
+  using P = host::Xyzz<host::Fp>;
+  const uint32_t* raw = reinterpret_cast<const uint32_t*>(h_windows);
+  P acc = P::inf();
+  for (int w = W - 1; w >= 0; w--) {
+    for (int i = 0; i < c; i++) acc = acc.dbl();
+    const uint32_t* q = raw + (size_t)w * 32;
+    P win{fp_from_words(q), fp_from_words(q + 8), fp_from_words(q + 16), fp_from_words(q + 24)};
+    acc = acc.add(win);
+  }
+  host::Fp x, y;
+  const bool inf = acc.to_affine(x, y);
+  memcpy(out, x.v, 32);
+  memcpy(out + 4, y.v, 32);
+  return inf;
+}
+
+bool msm_g2_combine(const void* h_windows, int W, int c, uint64_t out[16]) {
+  using P = host::Xyzz<host::Fp2>;
+  const uint32_t* raw = reinterpret_cast<const uint32_t*>(h_windows);
+  auto f2 = [](const uint32_t* q) { return host::Fp2{fp_from_words(q), fp_from_words(q + 8)}; };
+  P acc = P::inf();
+  for (int w = W - 1; w >= 0; w--) {
+    for (int i = 0; i < c; i++) acc = acc.dbl();
+    const uint32_t* q = raw + (size_t)w * 64;
+    P win{f2(q), f2(q + 16), f2(q + 32), f2(q + 48)};
+    acc = acc.add(win);
+  }
+  host::Fp2 x, y;
+  const bool inf = acc.to_affine(x, y);
+  memcpy(out, x.c0.v, 32);
+  memcpy(out + 4, x.c1.v, 32);
+  memcpy(out + 8, y.c0.v, 32);
+  memcpy(out + 12, y.c1.v, 32);
+  return inf;
+}
+
+bool msm_g1_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t st, uint64_t out[8]) {
+  scratch.ensure(msm_scratch_bytes(n, false, cfg));
+  const void* dw;
+  int c;
+  const int W = msm_g1_enqueue(px, py, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
+  std::vector<uint8_t> h((size_t)W * 128);
+  ZK_CUDA(cudaMemcpyAsync(h.data(), dw, h.size(), cudaMemcpyDeviceToHost, st));
+  ZK_CUDA(cudaStreamSynchronize(st));
+  return msm_g1_combine(h.data(), W, c, out);
+}
+
+bool msm_g2_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t st, uint64_t out[16]) {
+  scratch.ensure(msm_scratch_bytes(n, true, cfg));
+  const void* dw;
+  int c;
+  const int W = msm_g2_enqueue(px, py, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
+  std::vector<uint8_t> h((size_t)W * 256);
+  ZK_CUDA(cudaMemcpyAsync(h.data(), dw, h.size(), cudaMemcpyDeviceToHost, st));
+  ZK_CUDA(cudaStreamSynchronize(st));
+  return msm_g2_combine(h.data(), W, c, out);
+}
+
+}  // namespace zk

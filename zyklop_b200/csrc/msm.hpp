@@ -1,0 +1,65 @@
+// Pippenger multi-scalar multiplication on G1 and G2 (host-side interface).
+//
+// Replaces the reference's msm_g1 (include/msm_g1.cuh:714-926) and
+// msm_g2_device (include/msm_g2.cuh:669-854): same inputs (SoA affine
+// Montgomery points with (0,0) = infinity, canonical scalars) and the same
+// affine Montgomery result, computed by a different GPU design:
+//
+//   1. msm_hist     signed c-bit digits of every scalar, warp-aggregated
+//                   per-(window, bucket) counts;
+//   2. msm_scan     exclusive scan of the counts (bucket offsets);
+//   3. msm_scatter  counting-sort of (point, sign) records by bucket;
+//   4. msm_accum    load-balanced segmented reduction: each thread adds a
+//                   fixed number K of consecutive sorted records with mixed
+//                   XYZZ+affine additions, so a bucket's size never decides a
+//                   thread's work (skewed scalars stay balanced); buckets that
+//                   cross thread ranges leave partial sums that further levels
+//                   of the same kernel combine;
+//   5. msm_bucket_reduce / msm_window_reduce
+//                   sum_b (b+1) S_b per window from chunked running sums;
+//   6. host         Horner over windows (latency-bound, done on one CPU core)
+//                   and affine conversion.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "runtime.hpp"
+
+namespace zk {
+
+struct MsmConfig {
+  int c = 0;          // window bits (0 = choose from n)
+  int k0 = 32;        // sorted records per thread in the first accumulation level
+  int k1 = 16;        // partial records per thread in later levels
+  int chunk = 16;     // buckets per thread in the bucket reduction
+};
+
+int msm_default_c(size_t n, bool g2);
+
+// Device scratch bytes one MSM of n points needs with this configuration.
+size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg);
+
+// Enqueue the GPU part of an MSM on `stream`; the W window sums (XYZZ) land
+// in the returned device pointer inside `scratch`.  `scratch` must hold
+// msm_scratch_bytes(n, ...) bytes.  Returns the number of windows.
+int msm_g1_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                   void* scratch, size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
+                   const void** d_windows, int* c_out);
+int msm_g2_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                   void* scratch, size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
+                   const void** d_windows, int* c_out);
+
+// Host combination of W window sums (XYZZ, as copied from the device) into an
+// affine Montgomery point.  Returns true for the point at infinity.
+bool msm_g1_combine(const void* h_windows, int n_windows, int c, uint64_t out[8]);
+bool msm_g2_combine(const void* h_windows, int n_windows, int c, uint64_t out[16]);
+
+// Blocking convenience wrappers: enqueue, copy the window sums back, combine.
+bool msm_g1_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t stream, uint64_t out[8]);
+bool msm_g2_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
+                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t stream, uint64_t out[16]);
+
+}  // namespace zk

@@ -1,0 +1,339 @@
+// Fr NTT / INTT and the H-polynomial pipeline on sm_100a (see ntt.hpp).
+// Reference counterparts: nttPrepare / twiddle builders
+// (include/ntt_bn254.cuh:166-261), ntt_stockham_fwd/inv + ntt_scale
+// (include/ntt_bn254.cuh:300-464), computeHPoly and its glue kernels
+// (src/groth16.cu:174-183, 914-948, 1037-1128).
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "field.cuh"
+#include "host_field.hpp"
+#include "ntt.hpp"
+
+namespace zk {
+namespace {
+
+constexpr int kTile = 1024;       // elements per pass tile
+constexpr int kPassThreads = 256;
+constexpr int kMaxPassBits = 8;   // radix-2^8 sub-transforms per pass
+
+using host::Fr;
+
+// omega_{2^lg} in Montgomery form: 5^((r-1)/2^28) squared (28 - lg) times
+Fr host_root(int lg) {
+  uint64_t e[4];
+  memcpy(e, host::FR_PARAMS.p, 32);
+  e[0] -= 1;
+  for (int i = 0; i < 28; i++) {
+    e[0] = (e[0] >> 1) | (e[1] << 63);
+    e[1] = (e[1] >> 1) | (e[2] << 63);
+    e[2] = (e[2] >> 1) | (e[3] << 63);
+    e[3] >>= 1;
+  }
+  Fr w = Fr::from_u64(5).pow(e);
+  for (int i = lg; i < 28; i++) w = w.sqr();
+  return w;
+}
+
+__global__ void k_tw_fill(fr_t* __restrict__ out, const fr_t* __restrict__ hi,
+                          const fr_t* __restrict__ lo, int lo_bits, size_t n) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const fr_t a = fe_load<FrCfg>(hi, e >> lo_bits);
+  const fr_t b = fe_load<FrCfg>(lo, e & ((size_t(1) << lo_bits) - 1));
+  fe_store(out, e, a * b);
+}
+
+struct PassArgs {
+  fr_t* in[3];
+  fr_t* out[3];
+};
+
+// One pass: radix-2 stages on global index bits [lo, lo + k) for every
+// sub-transform, in shared memory.  DIF runs the bits high -> low with
+// butterflies (u + v, (u - v) w); DIT runs low -> high with (u + v w, u - v w).
+// In both, the butterfly on bit b of pair (i, i + 2^b) uses
+// w^((i mod 2^b) << (L - 1 - b)).
+template <bool DIT>
+__global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const fr_t* __restrict__ tw,
+                                                           int tw_shift, int L, int lo, int k,
+                                                           int log_g) {
+  extern __shared__ uint32_t sm[];
+  const int tile = 1 << (k + log_g);
+  const int G = 1 << log_g;
+  const fr_t* in = args.in[blockIdx.y];
+  fr_t* out = args.out[blockIdx.y];
+  const size_t gid0 = (size_t)blockIdx.x << log_g;
+  const size_t lomask = (size_t(1) << lo) - 1;
+  for (int e = threadIdx.x; e < tile; e += blockDim.x) {
+    int j, g;
+    if (lo == 0) {
+      j = e & ((1 << k) - 1);
+      g = e >> k;
+    } else {
+      g = e & (G - 1);
+      j = e >> log_g;
+    }
+    const size_t gid = gid0 + g;
+    const size_t idx = ((gid >> lo) << (lo + k)) | ((size_t)j << lo) | (gid & lomask);
+    const fr_t x = fe_load<FrCfg>(in, idx);
+    const int slot = (j << log_g) | g;
+#pragma unroll
+    for (int w = 0; w < 8; w++) sm[w * tile + slot] = x.v[w];
+  }
+  __syncthreads();
+  for (int st = 0; st < k; st++) {
+    const int bit = DIT ? st : (k - 1 - st);
+    const int gbit = lo + bit;
+    for (int bf = threadIdx.x; bf < tile / 2; bf += blockDim.x) {
+      const int g = bf & (G - 1);
+      const int jb = bf >> log_g;
+      const int jlo = jb & ((1 << bit) - 1), jhi = jb >> bit;
+      const int j0 = (jhi << (bit + 1)) | jlo;
+      const int s0 = (j0 << log_g) | g;
+      const int s1 = s0 | (1 << (bit + log_g));
+      const size_t gid = gid0 + g;
+      const size_t imod = ((size_t)jlo << lo) | (gid & lomask);
+      const fr_t w = fe_ldg<FrCfg>(tw, (imod << (L - 1 - gbit)) << tw_shift);
+      fr_t u, v;
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        u.v[q] = sm[q * tile + s0];
+        v.v[q] = sm[q * tile + s1];
+      }
+      fr_t a, b;
+      if (DIT) {
+        v = v * w;
+        a = u + v;
+        b = u - v;
+      } else {
+        a = u + v;
+        b = (u - v) * w;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        sm[q * tile + s0] = a.v[q];
+        sm[q * tile + s1] = b.v[q];
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < tile; e += blockDim.x) {
+    int j, g;
+    if (lo == 0) {
+      j = e & ((1 << k) - 1);
+      g = e >> k;
+    } else {
+      g = e & (G - 1);
+      j = e >> log_g;
+    }
+    const size_t gid = gid0 + g;
+    const size_t idx = ((gid >> lo) << (lo + k)) | ((size_t)j << lo) | (gid & lomask);
+    const int slot = (j << log_g) | g;
+    fr_t x;
+#pragma unroll
+    for (int w = 0; w < 8; w++) x.v[w] = sm[w * tile + slot];
+    fe_store(out, idx, x);
+  }
+}
+
+__global__ void k_bitrev(const fr_t* __restrict__ in, fr_t* __restrict__ out, int L, bool scale,
+                         fr_t factor) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >> L) return;
+  const size_t r = L ? (__brevll((unsigned long long)i) >> (64 - L)) : 0;
+  fr_t x = fe_load<FrCfg>(in, i);
+  if (scale) x = x * factor;
+  fe_store(out, r, x);
+}
+
+__global__ void k_pointwise_mul(const fr_t* __restrict__ a, const fr_t* __restrict__ b,
+                                fr_t* __restrict__ c, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) fe_store(c, i, fe_load<FrCfg>(a, i) * fe_load<FrCfg>(b, i));
+}
+
+// x[p] *= (1/N) omega_2n^rev(p) for coefficients held in bit-reversed order
+// (the coset shift of src/groth16.cu:914-921 with the INTT scale folded in).
+__global__ void k_coset_scale(PassArgs args, const fr_t* __restrict__ tw, int tw_shift, int L,
+                              fr_t c_even, fr_t c_odd) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >> L) return;
+  fr_t* a = args.in[blockIdx.y];
+  const size_t e = L ? (__brevll((unsigned long long)p) >> (64 - L)) : 0;
+  const size_t f = e >> 1;  // omega_2n^e = omega_2n^(e & 1) * omega_N^f
+  const size_t half = L ? (size_t(1) << (L - 1)) : 1;
+  fr_t t;
+  if (f < half) {
+    t = fe_ldg<FrCfg>(tw, f << tw_shift);
+  } else {
+    t = fe_neg(fe_ldg<FrCfg>(tw, (f - half) << tw_shift));  // omega_N^(N/2) = -1
+  }
+  fe_store(a, p, fe_load<FrCfg>(a, p) * t * ((e & 1) ? c_odd : c_even));
+}
+
+// h = A*B - C, decoded to canonical (src/groth16.cu:935-948, 218-226)
+__global__ void k_h_final(const fr_t* __restrict__ a, const fr_t* __restrict__ b,
+                          const fr_t* __restrict__ c, fr_t* __restrict__ h, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const fr_t v = fe_load<FrCfg>(a, i) * fe_load<FrCfg>(b, i) - fe_load<FrCfg>(c, i);
+  fe_store(h, i, fe_from_mont(v));
+}
+
+__global__ void k_fr_encode(const fr_t* __restrict__ in, fr_t* __restrict__ out, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) fe_store(out, i, fe_to_mont(fe_load<FrCfg>(in, i)));
+}
+__global__ void k_fr_decode(const fr_t* __restrict__ in, fr_t* __restrict__ out, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) fe_store(out, i, fe_from_mont(fe_load<FrCfg>(in, i)));
+}
+
+fr_t to_dev(const Fr& x) {
+  fr_t r;
+  memcpy(r.v, x.v, 32);
+  return r;
+}
+
+// Bit ranges [lo, lo + k) covering [0, L) in near-equal pieces of <= 8 bits.
+int split_passes(int L, int* lo, int* k) {
+  const int np = (L + kMaxPassBits - 1) / kMaxPassBits;
+  int at = 0;
+  for (int i = 0; i < np; i++) {
+    const int bits = (L - at) / (np - i);
+    lo[i] = at;
+    k[i] = bits;
+    at += bits;
+  }
+  return np;
+}
+
+void run_pass(bool dit, const PassArgs& args, int count, const fr_t* tw, int tw_shift, int L, int lo,
+              int k, cudaStream_t st) {
+  const size_t groups = size_t(1) << (L - k);
+  int log_g = 0;
+  while ((1 << (log_g + 1 + k)) <= kTile && (size_t(1) << (log_g + 1)) <= groups &&
+         (lo == 0 || log_g + 1 <= lo))
+    log_g++;
+  const size_t blocks = groups >> log_g;
+  const size_t smem = (size_t)8 * 4 * (size_t(1) << (k + log_g));
+  dim3 grid((unsigned)blocks, count);
+  if (dit)
+    k_ntt_pass<true><<<grid, kPassThreads, smem, st>>>(args, tw, tw_shift, L, lo, k, log_g);
+  else
+    k_ntt_pass<false><<<grid, kPassThreads, smem, st>>>(args, tw, tw_shift, L, lo, k, log_g);
+  ZK_CHECK_LAUNCH();
+}
+
+// all DIF passes (high bit ranges first); first pass may be out of place
+void dif(const PassArgs& first, const PassArgs& rest, int count, const fr_t* tw, int tw_shift, int L,
+         cudaStream_t st) {
+  int lo[8], k[8];
+  const int np = split_passes(L, lo, k);
+  for (int i = np - 1; i >= 0; i--)
+    run_pass(false, i == np - 1 ? first : rest, count, tw, tw_shift, L, lo[i], k[i], st);
+}
+
+void dit(const PassArgs& args, int count, const fr_t* tw, int tw_shift, int L, cudaStream_t st) {
+  int lo[8], k[8];
+  const int np = split_passes(L, lo, k);
+  for (int i = 0; i < np; i++) run_pass(true, args, count, tw, tw_shift, L, lo[i], k[i], st);
+}
+
+unsigned blocks_for(size_t n, int th = 256) { return (unsigned)((n + th - 1) / th); }
+
+}  // namespace
+
+void NttTables::ensure(int log_n, cudaStream_t st) {
+  ZK_REQUIRE(log_n >= 0 && log_n <= kMaxLogN, ZK_EINVAL, "ntt: log_n out of range");
+  const int need = log_n < 1 ? 1 : log_n;
+  if (lmax >= need) return;
+  const int lm = need;
+  const size_t half = size_t(1) << (lm - 1);
+  const int lo_bits = (lm - 1) < 12 ? (lm - 1) : 12;
+  const size_t nlo = size_t(1) << lo_bits, nhi = half >> lo_bits;
+  ZK_CUDA(cudaStreamSynchronize(st));
+  fwd.ensure(half * 32);
+  inv.ensure(half * 32);
+  DeviceBuffer tmp;
+  tmp.ensure((nlo + nhi) * 32 * 2);
+  for (int dir = 0; dir < 2; dir++) {
+    Fr w = host_root(lm);
+    if (dir) w = w.inv();
+    std::vector<Fr> lo_t(nlo), hi_t(nhi);
+    lo_t[0] = Fr::one();
+    for (size_t i = 1; i < nlo; i++) lo_t[i] = lo_t[i - 1] * w;
+    Fr step = nlo ? lo_t[nlo - 1] * w : w;  // w^nlo
+    hi_t[0] = Fr::one();
+    for (size_t i = 1; i < nhi; i++) hi_t[i] = hi_t[i - 1] * step;
+    char* base = tmp.as<char>() + dir * (nlo + nhi) * 32;
+    ZK_CUDA(cudaMemcpy(base, hi_t.data(), nhi * 32, cudaMemcpyHostToDevice));
+    ZK_CUDA(cudaMemcpy(base + nhi * 32, lo_t.data(), nlo * 32, cudaMemcpyHostToDevice));
+    fr_t* out = dir ? inv.as<fr_t>() : fwd.as<fr_t>();
+    k_tw_fill<<<blocks_for(half), 256, 0, st>>>(out, reinterpret_cast<const fr_t*>(base),
+                                                reinterpret_cast<const fr_t*>(base + nhi * 32),
+                                                lo_bits, half);
+    ZK_CHECK_LAUNCH();
+  }
+  ZK_CUDA(cudaStreamSynchronize(st));
+  lmax = lm;
+}
+
+void ntt_inplace(NttTables& tw, uint64_t* a, int log_n, bool inverse, void* scratch,
+                 cudaStream_t st) {
+  ZK_REQUIRE(log_n >= 0 && log_n <= kMaxLogN, ZK_EINVAL, "ntt: log_n out of range");
+  if (log_n == 0) return;
+  tw.ensure(log_n, st);
+  const int shift = tw.lmax - log_n;
+  const fr_t* table = inverse ? tw.inv.as<fr_t>() : tw.fwd.as<fr_t>();
+  fr_t* x = reinterpret_cast<fr_t*>(a);
+  fr_t* s = reinterpret_cast<fr_t*>(scratch);
+  PassArgs first{{x, nullptr, nullptr}, {s, nullptr, nullptr}};
+  PassArgs rest{{s, nullptr, nullptr}, {s, nullptr, nullptr}};
+  dif(first, rest, 1, table, shift, log_n, st);
+  const size_t n = size_t(1) << log_n;
+  fr_t factor{};
+  if (inverse) factor = to_dev(Fr::from_u64(n).inv());
+  k_bitrev<<<blocks_for(n), 256, 0, st>>>(s, x, log_n, inverse, factor);
+  ZK_CHECK_LAUNCH();
+}
+
+void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, uint64_t* h,
+           cudaStream_t st) {
+  ZK_REQUIRE(log_n >= 1 && log_n < kMaxLogN, ZK_EINVAL, "hpoly: log_n out of range");
+  tw.ensure(log_n, st);
+  const size_t n = size_t(1) << log_n;
+  const int shift = tw.lmax - log_n;
+  fr_t* A = reinterpret_cast<fr_t*>(aw);
+  fr_t* B = reinterpret_cast<fr_t*>(bw);
+  fr_t* C = reinterpret_cast<fr_t*>(cw);
+  k_pointwise_mul<<<blocks_for(n), 256, 0, st>>>(A, B, C, n);
+  ZK_CHECK_LAUNCH();
+  PassArgs abc{{A, B, C}, {A, B, C}};
+  dif(abc, abc, 3, tw.inv.as<fr_t>(), shift, log_n, st);
+  const Fr ninv = Fr::from_u64(n).inv();
+  const Fr c_odd = ninv * host_root(log_n + 1);
+  k_coset_scale<<<dim3(blocks_for(n), 3), 256, 0, st>>>(abc, tw.fwd.as<fr_t>(), shift, log_n,
+                                                        to_dev(ninv), to_dev(c_odd));
+  ZK_CHECK_LAUNCH();
+  dit(abc, 3, tw.fwd.as<fr_t>(), shift, log_n, st);
+  k_h_final<<<blocks_for(n), 256, 0, st>>>(A, B, C, reinterpret_cast<fr_t*>(h), n);
+  ZK_CHECK_LAUNCH();
+}
+
+void fr_encode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t st) {
+  if (!n) return;
+  k_fr_encode<<<blocks_for(n), 256, 0, st>>>(reinterpret_cast<const fr_t*>(in),
+                                             reinterpret_cast<fr_t*>(out), n);
+  ZK_CHECK_LAUNCH();
+}
+void fr_decode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t st) {
+  if (!n) return;
+  k_fr_decode<<<blocks_for(n), 256, 0, st>>>(reinterpret_cast<const fr_t*>(in),
+                                             reinterpret_cast<fr_t*>(out), n);
+  ZK_CHECK_LAUNCH();
+}
+
+}  // namespace zk

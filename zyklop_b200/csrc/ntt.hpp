@@ -1,0 +1,51 @@
+// Fr number-theoretic transforms and the Groth16 H-polynomial pipeline.
+//
+// Convention (identical results to the reference, include/ntt_bn254.cuh:
+// 190-464): natural-order DFT X[k] = sum_i x[i] w^(ik) with
+// w = omega_N = 5^((r-1)/N); the inverse uses w^-1 and scales by 1/N.
+// Elements are Montgomery Fr.
+//
+// Layout of the work: each transform runs as ceil(log N / 8) passes over HBM;
+// a pass loads tiles of up to 256-point sub-transforms (times a few adjacent
+// columns for coalescing) into shared memory, runs up to 8 radix-2 stages there
+// and writes back.  Decimation-in-frequency passes take natural order to
+// bit-reversed order, decimation-in-time passes the reverse, so the H
+// pipeline (INTT -> coset shift -> NTT) never permutes: it keeps coefficients
+// in bit-reversed order between the two transforms.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "runtime.hpp"
+
+namespace zk {
+
+constexpr int kMaxLogN = 27;  // Fr 2-adicity is 28; H needs omega_2n
+
+// Twiddle tables tw[e] = w^e (forward) and w^-e (inverse), e < 2^(lmax-1),
+// w a primitive 2^lmax-th root.  Smaller transforms read them with a stride.
+struct NttTables {
+  int lmax = -1;
+  DeviceBuffer fwd, inv;
+  void ensure(int log_n, cudaStream_t stream);
+};
+
+// In-place natural-order transform of 2^log_n elements (scratch: 32 << log_n
+// bytes of device memory).
+void ntt_inplace(NttTables& tw, uint64_t* a, int log_n, bool inverse, void* scratch,
+                 cudaStream_t stream);
+
+// H evaluations on the odd coset, following src/groth16.cu:1037-1090:
+//   C = A*B; a,b,c = INTT(A,B,C); x_i *= omega_2n^i; A',B',C' = NTT(a,b,c);
+//   h = A'B' - C' decoded to canonical.
+// aw and bw (Montgomery, 2^log_n each) are overwritten; cw is scratch of the
+// same size; h receives canonical Fr.
+void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, uint64_t* h,
+           cudaStream_t stream);
+
+// Elementwise helpers over Montgomery / canonical Fr arrays.
+void fr_encode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t stream);
+void fr_decode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t stream);
+
+}  // namespace zk
