@@ -107,6 +107,68 @@ int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk);
 /* Device scratch bytes an MSM of n points needs under the current config. */
 int zk_msm_scratch_bytes(zk_ctx* ctx, int group, size_t n, size_t* bytes);
 
+/* ---- Groth16 proving ------------------------------------------------------- */
+/* A circuit is a zkey made resident on the device: CRS points (sections 5-9,
+ * kept in their AoS zkey layout), A/B matrices as CSR built on the GPU from
+ * section 4, and the verification-key points.  It belongs to the context it
+ * was loaded on.  No reference counterpart: the reference re-reads the zkey in
+ * every groth16Prove call (src/groth16.cu:1143-1293). */
+typedef struct zk_circuit zk_circuit;
+int zk_circuit_load_file(zk_ctx* ctx, const char* zkey_path, zk_circuit** out);
+int zk_circuit_load_mem(zk_ctx* ctx, const uint8_t* zkey, size_t len, zk_circuit** out);
+int zk_circuit_free(zk_circuit* c);
+int zk_circuit_info(const zk_circuit* c, uint32_t* n_vars, uint32_t* n_public, uint32_t* domain);
+
+/* Proves with a witness of n_witness >= nVars canonical Fr values (wtns
+ * section 2 layout).  r, s: canonical Fr blinding scalars, or both NULL for
+ * the reference's unblinded proof (which is then bit-identical to the
+ * reference's).  proof: pi_A[8], pi_B[16], pi_C[8] u64, affine Montgomery,
+ * the layout of the reference's Groth16Proof (include/groth16.cuh:69-73).
+ * Replaces the proving part of groth16Prove (src/groth16.cu:1177-1389).
+ * zk_prove takes a host witness, zk_prove_device a device one. */
+int zk_prove(zk_circuit* c, const uint64_t* h_witness, size_t n_witness, const uint64_t* r,
+             const uint64_t* s, uint64_t* proof);
+int zk_prove_device(zk_circuit* c, const uint64_t* d_witness, size_t n_witness, const uint64_t* r,
+                    const uint64_t* s, uint64_t* proof);
+/* Unblinded proof that also copies out A.w, B.w (Montgomery, domain x 4 u64)
+ * and h (canonical, domain x 4 u64) into host buffers (any may be NULL).
+ * For checking the pipeline's intermediates. */
+int zk_prove_intermediates(zk_circuit* c, const uint64_t* h_witness, size_t n_witness,
+                           uint64_t* aw, uint64_t* bw, uint64_t* h, uint64_t* proof);
+
+/* One-shot proof from zkey + wtns files / in-memory images (the circuit is
+ * loaded, used and released inside the call).  Replaces
+ * groth16Prove(const char*, const char*, Groth16Proof&)
+ * (include/groth16.cuh:119-123, src/groth16.cu:1143-1397). */
+int zk_groth16_prove_files(zk_ctx* ctx, const char* zkey_path, const char* wtns_path,
+                           uint64_t* proof);
+int zk_groth16_prove_mem(zk_ctx* ctx, const uint8_t* zkey, size_t zkey_len, const uint8_t* wtns,
+                         size_t wtns_len, uint64_t* proof);
+
+/* Same fields as the reference's Groth16ZkeyHeader (include/groth16.cuh:79-86). */
+typedef struct {
+  uint32_t n_constraints; /* zkey domainSize field */
+  uint32_t n_vars;
+  uint32_t n_public;
+  uint32_t domain_size;   /* next power of two >= n_constraints */
+  int32_t log_domain;
+  uint64_t prime[4];      /* BN254 scalar field modulus */
+} zk_zkey_header;
+/* Replaces groth16ReadZkeyHeader (include/groth16.cuh:177-180). */
+int zk_read_zkey_header(const char* zkey_path, zk_zkey_header* hdr);
+
+/* snarkjs JSON text of a proof, the reference's exact format; needs
+ * out_size >= ~1100.  Replaces groth16ProofToSnarkjsJson
+ * (include/groth16.cuh:149-153, src/groth16.cu:1467-1502). */
+int zk_proof_to_json(const uint64_t* proof, char* out, size_t out_size);
+/* 256-byte EVM calldata (A.x, A.y, B.x.a1, B.x.a0, B.y.a1, B.y.a0, C.x, C.y,
+ * big-endian canonical).  Replaces groth16ProofToCalldata
+ * (include/groth16.cuh:163-167, src/groth16.cu:1509-1557). */
+int zk_proof_to_calldata(const uint64_t* proof, uint8_t* out, size_t out_size);
+/* public.json text (w[1..n_public] in decimal) from a wtns file.  Replaces
+ * writePublicJson (src/main.cu:28-110). */
+int zk_public_json(const char* wtns_path, uint32_t n_public, char* out, size_t out_size);
+
 /* ---- setup helpers --------------------------------------------------------- */
 /* d_px[i], d_py[i] = k_i * G (affine Montgomery) for the standard generator of
  * G1 (group 1; 4 u64 per coordinate) or G2 (group 2; 8 u64), k_i canonical
@@ -114,6 +176,26 @@ int zk_msm_scratch_bytes(zk_ctx* ctx, int group, size_t n, size_t* bytes);
  * from snarkjs; this builds seeded synthetic CRS points and MSM bases. */
 int zk_mul_generator(zk_ctx* ctx, int group, const uint64_t* d_scalars, size_t n, uint64_t* d_px,
                      uint64_t* d_py);
+
+/* Seeded synthetic Groth16 circuit + CRS, written as snarkjs-layout .zkey and
+ * .wtns files (sections 1-9; wtns version 2).  domain = 2^log_domain holds
+ * 2^log_domain - n_public - 1 multiplication gates plus the n_public + 1
+ * public-input rows; each gate's A and B rows have nnz_min..nnz_max nonzeros
+ * on earlier variables.  witness_kind 0: uniform Fr inputs, gate outputs are
+ * the products; 1: circom-like values (55% in {0,1}, 15% below 2^64, 30%
+ * uniform).  The CRS comes from toxic waste derived from `seed`.  No
+ * reference counterpart (the reference's circuits come from circom/snarkjs). */
+typedef struct {
+  uint32_t log_domain;
+  uint32_t n_public;
+  uint32_t n_private_inputs;
+  uint32_t nnz_min;
+  uint32_t nnz_max;
+  uint32_t witness_kind;
+  uint64_t seed;
+} zk_synth_params;
+int zk_synth_circuit(zk_ctx* ctx, const zk_synth_params* params, const char* zkey_path,
+                     const char* wtns_path);
 
 #ifdef __cplusplus
 }

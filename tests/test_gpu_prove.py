@@ -1,0 +1,220 @@
+"""End-to-end Groth16 parity on seeded synthetic circuits.
+
+Checks, on the same zkey / wtns files:
+  * the synthetic CRS is sound: the oracle's proofs pass the pairing check;
+  * the library's unblinded proof is bit-identical to the oracle's, and so
+    are the pipeline intermediates (A.w, B.w, h);
+  * blinded proofs equal the oracle's blinded proofs and verify;
+  * the library's proof equals the reference's own sm_100a build
+    (groth16Prove, src/groth16.cu:1143) and the CLI writes byte-identical
+    proof.json / public.json (src/main.cu);
+  * malformed inputs come back as status codes.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import _ref
+from _oracle import R
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+CIRCUITS = {
+    # name: (log_domain, witness kind, nnz range, seed)
+    "u10": (10, "uniform", (2, 2), 11),
+    "c10": (10, "circom", (1, 4), 12),
+    "u16": (16, "uniform", (2, 2), 13),
+}
+
+
+@pytest.fixture(scope="module")
+def api():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from zyklop_b200 import api as A
+    return A
+
+
+@pytest.fixture(scope="module")
+def files(api, tmp_path_factory):
+    d = tmp_path_factory.mktemp("circuits")
+    out = {}
+    for name, (lg, kind, nnz, seed) in CIRCUITS.items():
+        z, w = d / f"{name}.zkey", d / f"{name}.wtns"
+        api.synth_circuit(z, w, lg, n_public=8, n_private_inputs=8, nnz=nnz, witness=kind, seed=seed)
+        out[name] = (str(z), str(w))
+    return out
+
+
+def blob(path):
+    with open(path, "rb") as f:
+        return f.read()
+
+
+def publics(api, wtns, l):
+    w = api.read_wtns(wtns)
+    return [int.from_bytes(w[i].tobytes(), "little") for i in range(1, l + 1)]
+
+
+@pytest.mark.parametrize("name", ["u10", "c10"])
+def test_synthetic_crs_is_sound(api, oracle, files, name):
+    z, w = files[name]
+    zb, wb = blob(z), blob(w)
+    pub = publics(api, w, 8)
+    proof = oracle.prove(zb, wb)
+    assert oracle.verify(zb, proof, pub) == 1
+    blinded = oracle.prove(zb, wb, r=12345, s=67890)
+    assert oracle.verify(zb, blinded, pub) == 1
+    bad = proof.copy()
+    bad[24:32] = blinded[24:32]  # mismatched C
+    assert oracle.verify(zb, bad, pub) == 0
+    assert oracle.verify(zb, proof, [pub[0] + 1] + pub[1:]) == 0
+
+
+@pytest.mark.parametrize("name", ["u10", "c10", "u16"])
+def test_prove_matches_oracle(api, oracle, files, name):
+    z, w = files[name]
+    c = api.Circuit(z)
+    mine = c.prove(api.read_wtns(w))
+    assert np.array_equal(mine, oracle.prove(blob(z), blob(w)))
+
+
+@pytest.mark.parametrize("name", ["u10", "c10"])
+def test_intermediates_match_oracle(api, oracle, files, name):
+    z, w = files[name]
+    c = api.Circuit(z)
+    aw, bw, h, proof = c.intermediates(api.read_wtns(w))
+    oaw, obw, oh = oracle.intermediates(blob(z), blob(w), c.domain)
+    assert np.array_equal(aw, oaw)
+    assert np.array_equal(bw, obw)
+    assert np.array_equal(h, oh)
+
+
+@pytest.mark.parametrize("name", ["u10", "c10"])
+def test_blinded_matches_oracle_and_verifies(api, oracle, files, name):
+    z, w = files[name]
+    rng = np.random.default_rng(3)
+    r = int.from_bytes(rng.bytes(32), "little") % R
+    s = int.from_bytes(rng.bytes(32), "little") % R
+    c = api.Circuit(z)
+    mine = c.prove(api.read_wtns(w), r=r, s=s)
+    assert np.array_equal(mine, oracle.prove(blob(z), blob(w), r=r, s=s))
+    assert oracle.verify(blob(z), mine, publics(api, w, 8)) == 1
+    # blinding changes the proof but not its validity
+    assert not np.array_equal(mine, c.prove(api.read_wtns(w)))
+
+
+def test_entry_points_agree(api, files):
+    z, w = files["u10"]
+    c = api.Circuit(z)
+    wit = api.read_wtns(w)
+    a = c.prove(wit)
+    assert np.array_equal(a, api.prove_files(z, w))
+    assert np.array_equal(a, api.prove_mem(blob(z), blob(w)))
+    d = api.to_device(wit)
+    assert np.array_equal(a, c.prove_device(d, wit.shape[0]))
+    # repeated proofs on the resident circuit are identical
+    assert np.array_equal(a, c.prove(wit))
+
+
+@pytest.mark.parametrize("name", ["u10", "c10", "u16"])
+def test_matches_reference_prover(api, files, name):
+    L = _ref.prove_lib()
+    if L is None:
+        pytest.skip("reference sm_100a build (oracle/_ref) not present")
+    z, w = files[name]
+    theirs = np.zeros(32, np.uint64)
+    assert L.zkref_prove_files(z.encode(), w.encode(),
+                               theirs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))) == 0
+    assert np.array_equal(api.prove_files(z, w), theirs)
+    buf = ctypes.create_string_buffer(4096)
+    L.zkref_proof_json(theirs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), buf, 4096)
+    assert api.proof_to_json(theirs) == buf.value.decode()
+
+
+def test_cli_matches_reference_cli(api, files, tmp_path):
+    ref_cli = os.path.join(ROOT, "oracle", "_ref", "prover")
+    my_cli = os.path.join(ROOT, "zyklop_b200", "bin", "prover")
+    z, w = files["u10"]
+    mine = subprocess.run([my_cli, z, w, str(tmp_path / "p1.json"), str(tmp_path / "q1.json")],
+                          capture_output=True, text=True, timeout=300)
+    assert mine.returncode == 0, mine.stderr
+    assert blob(tmp_path / "p1.json").decode() == api.proof_to_json(api.prove_files(z, w)) + "\n"
+    usage = subprocess.run([my_cli, z], capture_output=True, text=True, timeout=60)
+    assert usage.returncode == 1 and "Usage" in usage.stderr
+    if not os.path.exists(ref_cli):
+        pytest.skip("reference CLI not built")
+    ref = subprocess.run([ref_cli, z, w, str(tmp_path / "p2.json"), str(tmp_path / "q2.json")],
+                         capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stderr
+    assert blob(tmp_path / "p1.json") == blob(tmp_path / "p2.json")
+    assert blob(tmp_path / "q1.json") == blob(tmp_path / "q2.json")
+
+
+def test_cli_blinded_proof_verifies(api, oracle, files, tmp_path):
+    my_cli = os.path.join(ROOT, "zyklop_b200", "bin", "prover")
+    z, w = files["c10"]
+    out = subprocess.run([my_cli, z, w, str(tmp_path / "p.json"), str(tmp_path / "q.json"),
+                          "--blind", "7", "--repeat", "3"], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    import json
+    pj = json.loads(blob(tmp_path / "p.json"))
+    from _oracle import P, limbs, mont
+    def m(x):
+        return limbs(mont(int(x), P))
+    proof = np.concatenate([m(pj["pi_a"][0]), m(pj["pi_a"][1]), m(pj["pi_b"][0][0]),
+                            m(pj["pi_b"][0][1]), m(pj["pi_b"][1][0]), m(pj["pi_b"][1][1]),
+                            m(pj["pi_c"][0]), m(pj["pi_c"][1])])
+    pub = [int(x) for x in json.loads(blob(tmp_path / "q.json"))]
+    assert pub == publics(api, w, 8)
+    assert oracle.verify(blob(z), proof, pub) == 1
+
+
+def test_calldata_layout(api, files):
+    z, w = files["u10"]
+    proof = api.prove_files(z, w)
+    cd = api.proof_to_calldata(proof)
+    from _oracle import P, to_int, unmont
+    def be(i):
+        return int.from_bytes(cd[32 * i:32 * i + 32], "big")
+    assert be(0) == unmont(to_int(proof[0:4]), P) and be(1) == unmont(to_int(proof[4:8]), P)
+    assert be(2) == unmont(to_int(proof[12:16]), P) and be(3) == unmont(to_int(proof[8:12]), P)
+    assert be(6) == unmont(to_int(proof[24:28]), P)
+
+
+def test_header_and_public_json(api, files):
+    z, w = files["u10"]
+    h = api.read_zkey_header(z)
+    assert (h.domain_size, h.log_domain, h.n_public) == (1024, 10, 8)
+    text = api.public_json(w, 8)
+    assert text.startswith("[\n") and text.count(",") == 7
+
+
+def test_malformed_inputs_are_status_codes(api, files, tmp_path):
+    from zyklop_b200 import ZkError
+    z, w = files["u10"]
+    data = blob(z)
+    (tmp_path / "trunc.zkey").write_bytes(data[: len(data) // 2])
+    with pytest.raises(ZkError) as e:
+        api.prove_files(tmp_path / "trunc.zkey", w)
+    assert e.value.code == 5  # ZK_EFORMAT
+    (tmp_path / "magic.zkey").write_bytes(b"zkez" + data[4:])
+    with pytest.raises(ZkError) as e:
+        api.prove_files(tmp_path / "magic.zkey", w)
+    assert e.value.code == 5
+    with pytest.raises(ZkError) as e:
+        api.prove_files(tmp_path / "missing.zkey", w)
+    assert e.value.code == 4  # ZK_EIO
+    c = api.Circuit(z)
+    with pytest.raises(ZkError) as e:
+        c.prove(api.read_wtns(w)[:10])
+    assert e.value.code == 6  # ZK_EWITNESS
+    # the context stays usable after the failures
+    assert np.array_equal(c.prove(api.read_wtns(w)), api.prove_files(z, w))

@@ -41,7 +41,45 @@ SIGNATURES = {
                                             ctypes.POINTER(ctypes.c_size_t)]),
     "zk_mul_generator": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, sz,
                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "zk_circuit_load_file": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "zk_circuit_load_mem": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "zk_circuit_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "zk_circuit_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                       ctypes.POINTER(ctypes.c_uint32),
+                                       ctypes.POINTER(ctypes.c_uint32)]),
+    "zk_prove": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz, ctypes.c_void_p,
+                                ctypes.c_void_p, u64p]),
+    "zk_prove_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz, ctypes.c_void_p,
+                                       ctypes.c_void_p, u64p]),
+    "zk_prove_intermediates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              u64p]),
+    "zk_groth16_prove_files": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
+                                              u64p]),
+    "zk_groth16_prove_mem": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz, ctypes.c_void_p,
+                                            sz, u64p]),
+    "zk_read_zkey_header": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p]),
+    "zk_proof_to_json": (ctypes.c_int, [u64p, ctypes.c_char_p, sz]),
+    "zk_proof_to_calldata": (ctypes.c_int, [u64p, ctypes.c_void_p, sz]),
+    "zk_public_json": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_char_p, sz]),
+    "zk_synth_circuit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                                        ctypes.c_char_p]),
 }
+
+
+class ZkeyHeader(ctypes.Structure):
+    _fields_ = [("n_constraints", ctypes.c_uint32), ("n_vars", ctypes.c_uint32),
+                ("n_public", ctypes.c_uint32), ("domain_size", ctypes.c_uint32),
+                ("log_domain", ctypes.c_int32), ("prime", ctypes.c_uint64 * 4)]
+
+
+class SynthParams(ctypes.Structure):
+    _fields_ = [("log_domain", ctypes.c_uint32), ("n_public", ctypes.c_uint32),
+                ("n_private_inputs", ctypes.c_uint32), ("nnz_min", ctypes.c_uint32),
+                ("nnz_max", ctypes.c_uint32), ("witness_kind", ctypes.c_uint32),
+                ("seed", ctypes.c_uint64)]
 
 
 def lib():

@@ -101,3 +101,130 @@ def mul_generator(group, scalars, ctx=None, keep_on_device=False):
     if keep_on_device:
         return dx, dy
     return to_host(dx)[: w * n].reshape(n, w), to_host(dy)[: w * n].reshape(n, w)
+
+
+# ------------------------------------------------------------------ Groth16
+from ._lib import SynthParams, ZkeyHeader  # noqa: E402
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+def synth_circuit(zkey_path, wtns_path, log_domain, n_public=8, n_private_inputs=8, nnz=(2, 2),
+                  witness="uniform", seed=1, ctx=None):
+    """Write a seeded synthetic circuit + CRS (zkey) and its witness (wtns)."""
+    p = SynthParams(log_domain, n_public, n_private_inputs, nnz[0], nnz[1],
+                    {"uniform": 0, "circom": 1}[witness], seed)
+    check(lib().zk_synth_circuit(ctx, ctypes.byref(p), str(zkey_path).encode(),
+                                 str(wtns_path).encode()))
+
+
+def read_wtns(path):
+    """canonical witness values of a wtns file -> (n, 4) uint64"""
+    data = open(path, "rb").read()
+    assert data[:4] == b"wtns"
+    ns = int.from_bytes(data[8:12], "little")
+    pos, n_vars, values = 12, None, None
+    for _ in range(ns):
+        t = int.from_bytes(data[pos:pos + 4], "little")
+        size = int.from_bytes(data[pos + 4:pos + 12], "little")
+        pos += 12
+        if t == 1:
+            n_vars = int.from_bytes(data[pos + 36:pos + 40], "little")
+        elif t == 2:
+            values = data[pos:pos + size]
+        pos += size
+    return np.frombuffer(values, dtype=np.uint64)[: 4 * n_vars].reshape(n_vars, 4).copy()
+
+
+class Circuit:
+    """A zkey resident on the device (zk_circuit_load_file / zk_prove)."""
+
+    def __init__(self, zkey_path, ctx=None):
+        h = ctypes.c_void_p()
+        check(lib().zk_circuit_load_file(ctx, str(zkey_path).encode(), ctypes.byref(h)))
+        self.handle = h
+        a, b, c = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().zk_circuit_info(h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        self.n_vars, self.n_public, self.domain = a.value, b.value, c.value
+
+    def prove(self, witness, r=None, s=None):
+        w = np.ascontiguousarray(witness, dtype=np.uint64).reshape(-1, 4)
+        proof = np.zeros(32, dtype=np.uint64)
+        rr = np.array([(r >> (64 * i)) & (2**64 - 1) for i in range(4)], np.uint64) if r is not None else None
+        ss = np.array([(s >> (64 * i)) & (2**64 - 1) for i in range(4)], np.uint64) if s is not None else None
+        check(lib().zk_prove(self.handle, w.ctypes.data_as(ctypes.c_void_p), w.shape[0],
+                             rr.ctypes.data_as(ctypes.c_void_p) if rr is not None else None,
+                             ss.ctypes.data_as(ctypes.c_void_p) if ss is not None else None,
+                             proof.ctypes.data_as(_u64p)))
+        return proof
+
+    def prove_device(self, d_witness, n, r=None, s=None):
+        proof = np.zeros(32, dtype=np.uint64)
+        check(lib().zk_prove_device(self.handle, ptr(d_witness), n, None, None,
+                                    proof.ctypes.data_as(_u64p)))
+        return proof
+
+    def intermediates(self, witness):
+        w = np.ascontiguousarray(witness, dtype=np.uint64).reshape(-1, 4)
+        aw = np.zeros((self.domain, 4), np.uint64)
+        bw = np.zeros((self.domain, 4), np.uint64)
+        h = np.zeros((self.domain, 4), np.uint64)
+        proof = np.zeros(32, dtype=np.uint64)
+        check(lib().zk_prove_intermediates(self.handle, w.ctypes.data_as(ctypes.c_void_p),
+                                           w.shape[0], aw.ctypes.data_as(ctypes.c_void_p),
+                                           bw.ctypes.data_as(ctypes.c_void_p),
+                                           h.ctypes.data_as(ctypes.c_void_p),
+                                           proof.ctypes.data_as(_u64p)))
+        return aw, bw, h, proof
+
+    def close(self):
+        if self.handle:
+            lib().zk_circuit_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prove_files(zkey_path, wtns_path, ctx=None):
+    proof = np.zeros(32, dtype=np.uint64)
+    check(lib().zk_groth16_prove_files(ctx, str(zkey_path).encode(), str(wtns_path).encode(),
+                                       proof.ctypes.data_as(_u64p)))
+    return proof
+
+
+def prove_mem(zkey: bytes, wtns: bytes, ctx=None):
+    proof = np.zeros(32, dtype=np.uint64)
+    check(lib().zk_groth16_prove_mem(ctx, zkey, len(zkey), wtns, len(wtns),
+                                     proof.ctypes.data_as(_u64p)))
+    return proof
+
+
+def read_zkey_header(path):
+    h = ZkeyHeader()
+    check(lib().zk_read_zkey_header(str(path).encode(), ctypes.byref(h)))
+    return h
+
+
+def proof_to_json(proof):
+    buf = ctypes.create_string_buffer(4096)
+    p = np.ascontiguousarray(proof, dtype=np.uint64)
+    check(lib().zk_proof_to_json(p.ctypes.data_as(_u64p), buf, 4096))
+    return buf.value.decode()
+
+
+def proof_to_calldata(proof):
+    out = (ctypes.c_uint8 * 256)()
+    p = np.ascontiguousarray(proof, dtype=np.uint64)
+    check(lib().zk_proof_to_calldata(p.ctypes.data_as(_u64p), out, 256))
+    return bytes(out)
+
+
+def public_json(wtns_path, n_public):
+    size = 64 + 96 * (n_public + 1)
+    buf = ctypes.create_string_buffer(size)
+    check(lib().zk_public_json(str(wtns_path).encode(), n_public, buf, size))
+    return buf.value.decode()

@@ -5,6 +5,7 @@
 #include <mutex>
 #include <vector>
 
+#include "capi_util.hpp"
 #include "context.hpp"
 #include "field.cuh"
 
@@ -61,29 +62,7 @@ void use_device(zk_ctx* ctx) { ZK_CUDA(cudaSetDevice(ctx->device)); }
 
 using namespace zk;
 
-#define ZK_API_BEGIN try {
-#define ZK_API_END                                       \
-  }                                                      \
-  catch (const zk::Error& e) {                           \
-    zk::set_last_error(e.code, e.what());                \
-    return e.code;                                       \
-  }                                                      \
-  catch (const std::bad_alloc&) {                        \
-    zk::set_last_error(ZK_ENOMEM, "host allocation failed"); \
-    return ZK_ENOMEM;                                    \
-  }                                                      \
-  catch (const std::exception& e) {                      \
-    zk::set_last_error(ZK_EINTERNAL, e.what());          \
-    return ZK_EINTERNAL;                                 \
-  }                                                      \
-  zk::set_last_error(ZK_OK, "");                         \
-  return ZK_OK;
 
-static zk_ctx* resolve(zk_ctx* ctx) {
-  if (!ctx) return default_ctx();
-  use_device(ctx);
-  return ctx;
-}
 
 extern "C" {
 
@@ -122,7 +101,7 @@ int zk_ctx_destroy(zk_ctx* ctx) {
 
 int zk_ctx_sync(zk_ctx* ctx) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   ZK_CUDA(cudaStreamSynchronize(ctx->stream));
   ZK_API_END
 }
@@ -130,7 +109,7 @@ int zk_ctx_sync(zk_ctx* ctx) {
 int zk_field_op(zk_ctx* ctx, int field, int op, uint64_t* d_out, const uint64_t* d_a,
                 const uint64_t* d_b, size_t n) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(field == ZK_FIELD_FP || field == ZK_FIELD_FR, ZK_EINVAL, "zk_field_op: bad field");
   ZK_REQUIRE(op >= 0 && op <= ZK_OP_DECODE, ZK_EINVAL, "zk_field_op: bad op");
@@ -155,7 +134,7 @@ int zk_field_op(zk_ctx* ctx, int field, int op, uint64_t* d_out, const uint64_t*
 
 int zk_ntt(zk_ctx* ctx, uint64_t* d_a, uint32_t log_n, int inverse) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(d_a, ZK_EINVAL, "zk_ntt: NULL buffer");
   ZK_REQUIRE(log_n <= (uint32_t)kMaxLogN, ZK_EINVAL, "zk_ntt: log_n > 27");
@@ -167,7 +146,7 @@ int zk_ntt(zk_ctx* ctx, uint64_t* d_a, uint32_t log_n, int inverse) {
 
 int zk_hpoly(zk_ctx* ctx, uint64_t* d_aw, uint64_t* d_bw, uint32_t log_n, uint64_t* d_h) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(d_aw && d_bw && d_h, ZK_EINVAL, "zk_hpoly: NULL buffer");
   ZK_REQUIRE(log_n >= 1 && log_n < (uint32_t)kMaxLogN, ZK_EINVAL, "zk_hpoly: log_n out of range");
@@ -180,11 +159,11 @@ int zk_hpoly(zk_ctx* ctx, uint64_t* d_aw, uint64_t* d_bw, uint32_t log_n, uint64
 int zk_msm_g1(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
               size_t n, uint64_t* h_out, int* is_inf) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(h_out, ZK_EINVAL, "zk_msm_g1: NULL output");
   ZK_REQUIRE(n == 0 || (d_px && d_py && d_scalars), ZK_EINVAL, "zk_msm_g1: NULL input");
-  const bool inf = msm_g1_run(d_px, d_py, d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[0],
+  const bool inf = msm_g1_run(points_soa(d_px, d_py), d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[0],
                               ctx->stream, h_out);
   if (is_inf) *is_inf = inf ? 1 : 0;
   ZK_API_END
@@ -193,11 +172,11 @@ int zk_msm_g1(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uin
 int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
               size_t n, uint64_t* h_out, int* is_inf) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(h_out, ZK_EINVAL, "zk_msm_g2: NULL output");
   ZK_REQUIRE(n == 0 || (d_px && d_py && d_scalars), ZK_EINVAL, "zk_msm_g2: NULL input");
-  const bool inf = msm_g2_run(d_px, d_py, d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[1],
+  const bool inf = msm_g2_run(points_soa(d_px, d_py), d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[1],
                               ctx->stream, h_out);
   if (is_inf) *is_inf = inf ? 1 : 0;
   ZK_API_END
@@ -205,7 +184,7 @@ int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uin
 
 int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_msm_set_config: group must be 1 or 2");
   ZK_REQUIRE(c == 0 || (c >= 4 && c <= 21), ZK_EINVAL, "zk_msm_set_config: c must be 0 or 4..21");
@@ -222,7 +201,7 @@ int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk) 
 
 int zk_msm_scratch_bytes(zk_ctx* ctx, int group, size_t n, size_t* bytes) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   ZK_REQUIRE(bytes, ZK_EINVAL, "zk_msm_scratch_bytes: NULL output");
   ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_msm_scratch_bytes: group must be 1 or 2");
   *bytes = msm_scratch_bytes(n, group == 2, ctx->msm_cfg[group - 1]);
@@ -232,7 +211,7 @@ int zk_msm_scratch_bytes(zk_ctx* ctx, int group, size_t n, size_t* bytes) {
 int zk_mul_generator(zk_ctx* ctx, int group, const uint64_t* d_scalars, size_t n, uint64_t* d_px,
                      uint64_t* d_py) {
   ZK_API_BEGIN
-  ctx = resolve(ctx);
+  ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_mul_generator: group must be 1 or 2");
   ZK_REQUIRE(n == 0 || (d_scalars && d_px && d_py), ZK_EINVAL, "zk_mul_generator: NULL buffer");

@@ -1,0 +1,171 @@
+// C ABI of the Groth16 prover: circuits, proofs, files, serialization
+// (declared in include/zyklop_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "capi_util.hpp"
+#include "prover.hpp"
+#include "serialize.hpp"
+
+using namespace zk;
+
+
+
+
+extern "C" {
+
+int zk_circuit_load_file(zk_ctx* ctx, const char* zkey_path, zk_circuit** out) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(zkey_path && out, ZK_EINVAL, "zk_circuit_load_file: NULL argument");
+  *out = nullptr;
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  auto f = BinFile::open(zkey_path, "zkey", 1);
+  *out = circuit_load(ctx, *f);
+  ZK_API_END
+}
+
+int zk_circuit_load_mem(zk_ctx* ctx, const uint8_t* zkey, size_t len, zk_circuit** out) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(zkey && out, ZK_EINVAL, "zk_circuit_load_mem: NULL argument");
+  *out = nullptr;
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  auto f = BinFile::wrap(zkey, len, "zkey", 1);
+  *out = circuit_load(ctx, *f);
+  ZK_API_END
+}
+
+int zk_circuit_free(zk_circuit* c) {
+  ZK_API_BEGIN
+  if (!c) return ZK_OK;
+  zk_ctx* ctx = c->ctx;
+  use_device(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  delete c;
+  ZK_API_END
+}
+
+int zk_circuit_info(const zk_circuit* c, uint32_t* n_vars, uint32_t* n_public, uint32_t* domain) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(c, ZK_EINVAL, "zk_circuit_info: NULL circuit");
+  if (n_vars) *n_vars = c->m1;
+  if (n_public) *n_public = c->l;
+  if (domain) *domain = c->n;
+  ZK_API_END
+}
+
+int zk_prove(zk_circuit* c, const uint64_t* h_witness, size_t n_witness, const uint64_t* r,
+             const uint64_t* s, uint64_t* proof) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(c && proof, ZK_EINVAL, "zk_prove: NULL argument");
+  ZK_REQUIRE((r == nullptr) == (s == nullptr), ZK_EINVAL, "zk_prove: give both r and s or neither");
+  use_device(c->ctx);
+  std::lock_guard<std::mutex> g(c->ctx->mu);
+  prove(c, h_witness, n_witness, false, r, s, proof, nullptr);
+  ZK_API_END
+}
+
+int zk_prove_device(zk_circuit* c, const uint64_t* d_witness, size_t n_witness, const uint64_t* r,
+                    const uint64_t* s, uint64_t* proof) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(c && proof, ZK_EINVAL, "zk_prove_device: NULL argument");
+  ZK_REQUIRE((r == nullptr) == (s == nullptr), ZK_EINVAL,
+             "zk_prove_device: give both r and s or neither");
+  use_device(c->ctx);
+  std::lock_guard<std::mutex> g(c->ctx->mu);
+  prove(c, d_witness, n_witness, true, r, s, proof, nullptr);
+  ZK_API_END
+}
+
+int zk_prove_intermediates(zk_circuit* c, const uint64_t* h_witness, size_t n_witness,
+                           uint64_t* aw, uint64_t* bw, uint64_t* h, uint64_t* proof) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(c && proof, ZK_EINVAL, "zk_prove_intermediates: NULL argument");
+  use_device(c->ctx);
+  std::lock_guard<std::mutex> g(c->ctx->mu);
+  ProveIntermediates dbg;
+  dbg.aw = aw;
+  dbg.bw = bw;
+  dbg.h = h;
+  prove(c, h_witness, n_witness, false, nullptr, nullptr, proof, &dbg);
+  ZK_API_END
+}
+
+int zk_groth16_prove_mem(zk_ctx* ctx, const uint8_t* zkey, size_t zkey_len, const uint8_t* wtns,
+                         size_t wtns_len, uint64_t* proof) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(zkey && wtns && proof, ZK_EINVAL, "zk_groth16_prove_mem: NULL argument");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  auto zf = BinFile::wrap(zkey, zkey_len, "zkey", 1);
+  auto wf = BinFile::wrap(wtns, wtns_len, "wtns", 2);
+  const WtnsView w = parse_wtns(*wf);
+  std::unique_ptr<zk_circuit> c(circuit_load(ctx, *zf));
+  prove(c.get(), w.values, w.n_vars, false, nullptr, nullptr, proof, nullptr);
+  ZK_API_END
+}
+
+int zk_groth16_prove_files(zk_ctx* ctx, const char* zkey_path, const char* wtns_path,
+                           uint64_t* proof) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(zkey_path && wtns_path && proof, ZK_EINVAL, "zk_groth16_prove_files: NULL argument");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  auto zf = BinFile::open(zkey_path, "zkey", 1);
+  auto wf = BinFile::open(wtns_path, "wtns", 2);
+  const WtnsView w = parse_wtns(*wf);
+  std::unique_ptr<zk_circuit> c(circuit_load(ctx, *zf));
+  prove(c.get(), w.values, w.n_vars, false, nullptr, nullptr, proof, nullptr);
+  ZK_API_END
+}
+
+int zk_read_zkey_header(const char* zkey_path, zk_zkey_header* hdr) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(zkey_path && hdr, ZK_EINVAL, "zk_read_zkey_header: NULL argument");
+  auto zf = BinFile::open(zkey_path, "zkey", 1);
+  const ZkeyView z = parse_zkey(*zf);
+  hdr->n_constraints = z.domain_raw;
+  hdr->n_vars = z.n_vars;
+  hdr->n_public = z.n_public;
+  hdr->domain_size = z.domain;
+  hdr->log_domain = z.log_n;
+  const uint64_t r[4] = {0x43e1f593f0000001ULL, 0x2833e84879b97091ULL, 0xb85045b68181585dULL,
+                         0x30644e72e131a029ULL};
+  memcpy(hdr->prime, r, 32);
+  ZK_API_END
+}
+
+int zk_proof_to_json(const uint64_t* proof, char* out, size_t out_size) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(proof && out && out_size, ZK_EINVAL, "zk_proof_to_json: NULL argument");
+  const std::string s = proof_json(proof);
+  ZK_REQUIRE(s.size() + 1 <= out_size, ZK_EINVAL, "zk_proof_to_json: output buffer too small");
+  memcpy(out, s.c_str(), s.size() + 1);
+  ZK_API_END
+}
+
+int zk_proof_to_calldata(const uint64_t* proof, uint8_t* out, size_t out_size) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(proof && out, ZK_EINVAL, "zk_proof_to_calldata: NULL argument");
+  ZK_REQUIRE(out_size >= 256, ZK_EINVAL, "zk_proof_to_calldata: buffer smaller than 256 bytes");
+  proof_calldata(proof, out);
+  ZK_API_END
+}
+
+int zk_public_json(const char* wtns_path, uint32_t n_public, char* out, size_t out_size) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(wtns_path && out && out_size, ZK_EINVAL, "zk_public_json: NULL argument");
+  auto wf = BinFile::open(wtns_path, "wtns", 2);
+  const WtnsView w = parse_wtns(*wf);
+  ZK_REQUIRE(w.n_vars >= n_public + 1, ZK_EWITNESS, "witness has fewer than nPublic + 1 values");
+  const std::string s = public_json(w.values + 4, n_public);
+  ZK_REQUIRE(s.size() + 1 <= out_size, ZK_EINVAL, "zk_public_json: output buffer too small");
+  memcpy(out, s.c_str(), s.size() + 1);
+  ZK_API_END
+}
+
+}  // extern "C"

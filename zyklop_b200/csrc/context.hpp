@@ -8,6 +8,24 @@
 #include "ntt.hpp"
 #include "runtime.hpp"
 
+namespace zk {
+
+// Buffers and streams of one in-flight proof (reused across proofs).
+struct ProveWs {
+  static constexpr int kStreams = 5;  // 0: witness/SpMV/H/MSM_H, 1: A, 2: B2, 3: C, 4: B1
+  bool ready = false;
+  cudaStream_t st[kStreams] = {};
+  cudaEvent_t ev_we = nullptr;
+  cudaEvent_t ev_done[kStreams] = {};
+  DeviceBuffer we, aw, bw, cw, h;
+  DeviceBuffer msm[kStreams];
+  PinnedBuffer win[kStreams];
+  void init();
+  ~ProveWs();
+};
+
+}  // namespace zk
+
 struct zk_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -16,6 +34,8 @@ struct zk_ctx {
   zk::DeviceBuffer ntt_scratch;
   zk::DeviceBuffer msm_scratch;
   zk::MsmConfig msm_cfg[2];
+  zk::ProveWs ws;
+  zk::Stager stager;
   bool is_default = false;
 };
 

@@ -10,13 +10,13 @@
 #include "curve.cuh"
 #include "host_field.hpp"
 #include "msm.hpp"
+#include "scan.cuh"
 
 namespace zk {
 namespace {
 
 constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr uint32_t kNeg = 0x80000000u;
-constexpr int kScanTile = 4096;   // entries per scan block (1024 threads x 4)
 
 // ------------------------------------------------------------------ shape
 struct Shape {
@@ -82,7 +82,7 @@ Layout<F> carve(void* base, const Shape& s) {
   Carver cv(base);
   L.counts = cv.take<uint32_t>(s.entries);
   L.cursor = cv.take<uint32_t>(s.entries);
-  L.tiles = cv.take<uint32_t>((s.entries + kScanTile - 1) / kScanTile + 1);
+  L.tiles = cv.take<uint32_t>(scan::tile_count(s.entries) + 1);
   L.skey = cv.take<uint32_t>(s.records);
   L.sval = cv.take<uint32_t>(s.records);
   L.buckets = cv.take<xyzz<F>>((size_t)s.W * s.B);
@@ -175,79 +175,6 @@ __global__ void k_msm_scatter(const uint64_t* __restrict__ sc, size_t n, int c, 
       skey[pos] = key;
       sval[pos] = (uint32_t)i | (neg ? kNeg : 0u);
     }
-  }
-}
-
-// ----------------------------------------------------------------- scan
-// Exclusive scan of `entries` u32 counts in three steps: per-tile scan,
-// scan of tile sums, add tile bases (and copy into the scatter cursor).
-__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sm_warp, uint32_t& total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  uint32_t x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) sm_warp[wid] = x;
-  __syncthreads();
-  if (wid == 0) {
-    uint32_t t = lane < nw ? sm_warp[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
-      if (lane >= o) t += y;
-    }
-    if (lane < nw) sm_warp[lane] = t;
-  }
-  __syncthreads();
-  const uint32_t warp_base = wid ? sm_warp[wid - 1] : 0;
-  total = sm_warp[nw - 1];
-  __syncthreads();
-  return warp_base + x - v;
-}
-
-__global__ void __launch_bounds__(1024) k_scan_tiles(uint32_t* __restrict__ a, size_t n,
-                                                     uint32_t* __restrict__ tiles) {
-  __shared__ uint32_t sw[32];
-  const size_t base = (size_t)blockIdx.x * kScanTile + threadIdx.x * 4;
-  uint32_t v[4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) v[j] = base + j < n ? a[base + j] : 0;
-  const uint32_t sum = v[0] + v[1] + v[2] + v[3];
-  uint32_t total;
-  uint32_t run = block_excl_scan(sum, sw, total);
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    if (base + j < n) a[base + j] = run;
-    run += v[j];
-  }
-  if (threadIdx.x == 0) tiles[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(1024) k_scan_top(uint32_t* __restrict__ tiles, int nt) {
-  __shared__ uint32_t sw[32];
-  // up to 4096 tiles: 4 per thread
-  uint32_t v[4];
-  const int base = threadIdx.x * 4;
-#pragma unroll
-  for (int j = 0; j < 4; j++) v[j] = base + j < nt ? tiles[base + j] : 0;
-  uint32_t total;
-  uint32_t run = block_excl_scan(v[0] + v[1] + v[2] + v[3], sw, total);
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    if (base + j < nt) tiles[base + j] = run;
-    run += v[j];
-  }
-}
-
-__global__ void k_scan_add(uint32_t* __restrict__ a, uint32_t* __restrict__ cursor, size_t n,
-                           const uint32_t* __restrict__ tiles) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) {
-    const uint32_t v = a[i] + tiles[i / kScanTile];
-    a[i] = v;
-    cursor[i] = v;
   }
 }
 
@@ -375,7 +302,8 @@ __device__ __forceinline__ void seg_block_finish(SegNode<F>* sm, uint32_t key_be
 template <class F>
 __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
-    const uint32_t* __restrict__ total_p, const F* __restrict__ px, const F* __restrict__ py, int K,
+    const uint32_t* __restrict__ total_p, const F* __restrict__ px, const F* __restrict__ py,
+    uint32_t pstride, int K,
     xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
   constexpr int T = seg_threads<F>();
   __shared__ SegNode<F> sm[T];
@@ -402,8 +330,8 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
       }
       const uint32_t v = sval[p];
       const uint32_t idx = v & ~kNeg;
-      const F x = ld_pod(px + idx);
-      F y = ld_pod(py + idx);
+      const F x = ld_pod(px + (size_t)idx * pstride);
+      F y = ld_pod(py + (size_t)idx * pstride);
       if (!(fe_is_zero(x) && fe_is_zero(y))) {
         if (v & kNeg) y = fe_neg(y);
         acc = xyzz_madd(acc, x, y);
@@ -510,9 +438,9 @@ __global__ void __launch_bounds__(128) k_msm_window_reduce(const xyzz<F>* __rest
 
 // --------------------------------------------------------------- driver
 template <class F>
-int msm_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                void* scratch, size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t st,
-                const void** d_windows, int* c_out) {
+int msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t st, const void** d_windows,
+                int* c_out) {
   constexpr bool g2 = sizeof(F) == 64;
   ZK_REQUIRE(n < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
   const Shape s = make_shape(n, g2, cfg);
@@ -529,12 +457,7 @@ int msm_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars,
     k_msm_hist<<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
     ZK_CHECK_LAUNCH();
   }
-  const int nt = (int)((s.entries + kScanTile - 1) / kScanTile);
-  ZK_REQUIRE(nt <= 4096, ZK_EINVAL, "msm: bucket table too large for the scan");
-  k_scan_tiles<<<nt, 1024, 0, st>>>(L.counts, s.entries, L.tiles);
-  k_scan_top<<<1, 1024, 0, st>>>(L.tiles, nt);
-  k_scan_add<<<(unsigned)((s.entries + 255) / 256), 256, 0, st>>>(L.counts, L.cursor, s.entries, L.tiles);
-  ZK_CHECK_LAUNCH();
+  scan::exclusive(L.counts, L.cursor, s.entries, L.tiles, st);
   if (n) {
     const int th = 256;
     const unsigned g = (unsigned)((n + th - 1) / th);
@@ -542,13 +465,13 @@ int msm_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars,
     ZK_CHECK_LAUNCH();
   }
   const uint32_t* total_p = L.counts + (s.entries - 1);
-  const F* fx = reinterpret_cast<const F*>(px);
-  const F* fy = reinterpret_cast<const F*>(py);
+  const F* fx = reinterpret_cast<const F*>(pts.x);
+  const F* fy = reinterpret_cast<const F*>(pts.y);
   // level 0
   {
     uint32_t* ok = s.levels > 1 ? L.pkey[1] : nullptr;
     k_msm_accum0<F><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
-        L.skey, L.sval, total_p, fx, fy, s.k0, L.buckets, ok, L.ppt[1]);
+        L.skey, L.sval, total_p, fx, fy, pts.stride, s.k0, L.buckets, ok, L.ppt[1]);
     ZK_CHECK_LAUNCH();
   }
   for (int l = 1; l < s.levels; l++) {
@@ -588,15 +511,15 @@ size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg) {
   return carve<fp_t>(nullptr, s).bytes;
 }
 
-int msm_g1_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                   void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st,
-                   const void** d_windows, int* c_out) {
-  return msm_enqueue<fp_t>(px, py, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
+int msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                   size_t bytes, const MsmConfig& cfg, cudaStream_t st, const void** d_windows,
+                   int* c_out) {
+  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
 }
-int msm_g2_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                   void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st,
-                   const void** d_windows, int* c_out) {
-  return msm_enqueue<fp2_t>(px, py, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
+int msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                   size_t bytes, const MsmConfig& cfg, cudaStream_t st, const void** d_windows,
+                   int* c_out) {
+  return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
 }
 
 namespace {
@@ -644,24 +567,24 @@ bool msm_g2_combine(const void* h_windows, int W, int c, uint64_t out[16]) {
   return inf;
 }
 
-bool msm_g1_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t st, uint64_t out[8]) {
+bool msm_g1_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,
+                const MsmConfig& cfg, cudaStream_t st, uint64_t out[8]) {
   scratch.ensure(msm_scratch_bytes(n, false, cfg));
   const void* dw;
   int c;
-  const int W = msm_g1_enqueue(px, py, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
+  const int W = msm_g1_enqueue(pts, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
   std::vector<uint8_t> h((size_t)W * 128);
   ZK_CUDA(cudaMemcpyAsync(h.data(), dw, h.size(), cudaMemcpyDeviceToHost, st));
   ZK_CUDA(cudaStreamSynchronize(st));
   return msm_g1_combine(h.data(), W, c, out);
 }
 
-bool msm_g2_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t st, uint64_t out[16]) {
+bool msm_g2_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,
+                const MsmConfig& cfg, cudaStream_t st, uint64_t out[16]) {
   scratch.ensure(msm_scratch_bytes(n, true, cfg));
   const void* dw;
   int c;
-  const int W = msm_g2_enqueue(px, py, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
+  const int W = msm_g2_enqueue(pts, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
   std::vector<uint8_t> h((size_t)W * 256);
   ZK_CUDA(cudaMemcpyAsync(h.data(), dw, h.size(), cudaMemcpyDeviceToHost, st));
   ZK_CUDA(cudaStreamSynchronize(st));

@@ -36,6 +36,19 @@ struct MsmConfig {
   int chunk = 16;     // buckets per thread in the bucket reduction
 };
 
+// Affine input points: x of point i at x + i*stride coordinates, y likewise.
+// stride 1 = separate x / y arrays (the reference's SoA msm_g1 arguments);
+// stride 2 = interleaved (x, y) records as stored in zkey sections 5-9.
+struct PointsView {
+  const void* x;
+  const void* y;
+  uint32_t stride;
+};
+inline PointsView points_soa(const void* px, const void* py) { return {px, py, 1}; }
+inline PointsView points_aos(const void* base, bool g2) {
+  return {base, reinterpret_cast<const char*>(base) + (g2 ? 64 : 32), 2};
+}
+
 int msm_default_c(size_t n, bool g2);
 
 // Device scratch bytes one MSM of n points needs with this configuration.
@@ -44,11 +57,11 @@ size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg);
 // Enqueue the GPU part of an MSM on `stream`; the W window sums (XYZZ) land
 // in the returned device pointer inside `scratch`.  `scratch` must hold
 // msm_scratch_bytes(n, ...) bytes.  Returns the number of windows.
-int msm_g1_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                   void* scratch, size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
+int msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                   size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
                    const void** d_windows, int* c_out);
-int msm_g2_enqueue(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                   void* scratch, size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
+int msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                   size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
                    const void** d_windows, int* c_out);
 
 // Host combination of W window sums (XYZZ, as copied from the device) into an
@@ -57,9 +70,9 @@ bool msm_g1_combine(const void* h_windows, int n_windows, int c, uint64_t out[8]
 bool msm_g2_combine(const void* h_windows, int n_windows, int c, uint64_t out[16]);
 
 // Blocking convenience wrappers: enqueue, copy the window sums back, combine.
-bool msm_g1_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t stream, uint64_t out[8]);
-bool msm_g2_run(const uint64_t* px, const uint64_t* py, const uint64_t* scalars, size_t n,
-                DeviceBuffer& scratch, const MsmConfig& cfg, cudaStream_t stream, uint64_t out[16]);
+bool msm_g1_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,
+                const MsmConfig& cfg, cudaStream_t stream, uint64_t out[8]);
+bool msm_g2_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,
+                const MsmConfig& cfg, cudaStream_t stream, uint64_t out[16]);
 
 }  // namespace zk

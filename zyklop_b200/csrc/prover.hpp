@@ -1,0 +1,57 @@
+// Groth16 prover: device-resident circuit + proving pipeline.
+//
+// Replaces groth16Prove (src/groth16.cu:1143-1397).  The same algebra:
+//   pi_A = MSM_G1([alpha1, A_0..A_m], [1, w_0..w_m])
+//   pi_B = MSM_G2([beta2, B2_0..B2_m], [1, w_0..w_m])
+//   pi_C = MSM_G1(C, w_{l+1..m}) + MSM_G1(H, h)
+// with h from the section-4 SpMV and the coset H pipeline, and optional
+// blinding r, s (which the reference omits): A += r delta1, B += s delta2,
+// C += s A + r B1 - r s delta1 with B1 = beta1 + sum w_i B1_i + s delta1.
+//
+// What changes is the organisation: the circuit (CSR matrices built on the
+// GPU from the raw section-4 bytes, CRS points in their zkey AoS layout) is
+// uploaded once and stays resident; a proof uploads only its witness; the
+// four MSMs run concurrently on their own streams while SpMV -> H -> MSM_H
+// runs on a fifth, instead of the reference's sequential, allocating calls.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "context.hpp"
+#include "zkey.hpp"
+
+struct zk_circuit {
+  zk_ctx* ctx = nullptr;
+  uint32_t m1 = 0, l = 0, n = 0;  // nVars, nPublic, domain
+  int log_n = 0;
+  uint32_t n_coefs = 0;
+  uint64_t alpha1[8], beta1[8], beta2[16], gamma2[16], delta1[8], delta2[16];
+  std::vector<uint64_t> ic;  // (l + 1) x 8, empty if the zkey has no section 3
+  bool has_b1 = false;
+  // CRS points, AoS (x, y) records; A / B1 / B2 carry alpha1 / beta1 / beta2
+  // as record 0, like the reference's extended buffers (src/groth16.cu:1199-1227)
+  zk::DeviceBuffer pts_a, pts_b1, pts_b2, pts_c, pts_h;
+  // CSR of the A and B matrices: row pointers (n + 1), signal ids, coef * R^2
+  zk::DeviceBuffer row[2], sig[2], val[2];
+};
+
+namespace zk {
+
+// Loads a circuit from a parsed zkey (uploads and builds the CSR on the
+// context's stream; blocks until done).
+zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& zkey);
+
+struct ProveIntermediates {
+  uint64_t* aw = nullptr;  // host, domain x 4 (Montgomery A.w)
+  uint64_t* bw = nullptr;  // host, domain x 4 (Montgomery B.w)
+  uint64_t* h = nullptr;   // host, domain x 4 (canonical h)
+};
+
+// Proves with a witness of >= m1 canonical Fr values (host or device memory).
+// r / s: canonical Fr blinding scalars or nullptr (reference behaviour).
+void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool witness_on_device,
+           const uint64_t* r, const uint64_t* s, uint64_t proof[32], ProveIntermediates* dbg);
+
+}  // namespace zk

@@ -49,6 +49,57 @@ void DeviceBuffer::release() {
   cap = 0;
 }
 
+void PinnedBuffer::ensure(size_t bytes) {
+  if (bytes <= cap && ptr) return;
+  release();
+  const size_t want = align256(bytes ? bytes : 256);
+  cudaError_t e = cudaMallocHost(&ptr, want);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    (void)cudaGetLastError();
+    throw Error(ZK_ENOMEM, std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
+  }
+  cap = want;
+}
+
+void PinnedBuffer::release() {
+  if (ptr) cudaFreeHost(ptr);
+  ptr = nullptr;
+  cap = 0;
+}
+
+Stager::~Stager() {
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+}
+
+void Stager::upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (!bytes) return;
+  for (int i = 0; i < 2; i++) {
+    buf[i].ensure(kChunk);
+    if (!ev[i]) ZK_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+  }
+  const char* s = reinterpret_cast<const char*>(src);
+  char* d = reinterpret_cast<char*>(dst);
+  for (size_t off = 0, k = 0; off < bytes; off += kChunk, k++) {
+    const size_t len = bytes - off < kChunk ? bytes - off : kChunk;
+    const int b = (int)(k & 1);
+    ZK_CUDA(cudaEventSynchronize(ev[b]));  // previous DMA from this buffer is done
+    char* p = buf[b].as<char>();
+    const long parts = (long)((len + (size_t(1) << 20) - 1) >> 20);
+#pragma omp parallel for schedule(static) num_threads(8)
+    for (long q = 0; q < parts; q++) {
+      const size_t o = (size_t)q << 20;
+      const size_t l = len - o < (size_t(1) << 20) ? len - o : (size_t(1) << 20);
+      memcpy(p + o, s + off + o, l);
+    }
+    ZK_CUDA(cudaMemcpyAsync(d + off, p, len, cudaMemcpyHostToDevice, st));
+    ZK_CUDA(cudaEventRecord(ev[b], st));
+  }
+  ZK_CUDA(cudaEventSynchronize(ev[0]));
+  ZK_CUDA(cudaEventSynchronize(ev[1]));
+}
+
 int device_sm_count() {
   int dev = 0, n = 0;
   cudaGetDevice(&dev);

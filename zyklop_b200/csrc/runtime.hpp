@@ -58,6 +58,32 @@ struct DeviceBuffer {
   T* as() const { return reinterpret_cast<T*>(ptr); }
 };
 
+// Growable page-locked host allocation (for asynchronous copies).
+struct PinnedBuffer {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer&) = delete;
+  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+  ~PinnedBuffer() { release(); }
+  void ensure(size_t bytes);
+  void release();
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+// Host -> device copy of pageable memory (a mapped file, a caller buffer)
+// through two pinned staging buffers: the CPU fills one chunk (with several
+// threads) while the DMA engine drains the other.  Blocks until the source
+// may be released; the device copy completes in stream order.
+struct Stager {
+  static constexpr size_t kChunk = size_t(32) << 20;
+  PinnedBuffer buf[2];
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  ~Stager();
+  void upload(void* dst, const void* src, size_t bytes, cudaStream_t st);
+};
+
 // Bump-pointer carve-out of a DeviceBuffer (256-byte aligned slices).
 struct Carver {
   char* base;
