@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Groth16 (BN254) proving throughput on B200.
+
+One step = one Groth16 proof of a seeded synthetic circuit with 2^20
+constraints (config-0 circuit shape: 2 nonzeros per A/B row, 8 public
+inputs, uniform witness), produced by libzyklop_b200.so.
+
+  value  proofs/s with the circuit resident in HBM and the witness already on
+         the device (zk_prove_device), CUDA events on the context stream,
+         max over ranks;
+  e2e    proofs/s through the reference-facing one-shot call
+         zk_groth16_prove_files(zkey, wtns) -- the drop-in for the reference's
+         groth16Prove -- which reads both files from the page cache and
+         uploads the CRS, matrices and witness inside the timed region;
+  roofline  the dominant kernel (MSM bucket accumulation) against the
+         measured IMAD throughput of the device;
+  cpu_baseline  the CPU oracle (C + OpenMP, every host thread) proving the
+         same circuit once.
+
+--impl reference runs the reference's own sm_100a build (oracle/_ref,
+compiled from the reference sources) through its groth16Prove on the same
+files.  With torchrun, every rank proves independently (replicas; the prover
+is single-GPU by design).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--log-domain L]
+"""
+import argparse
+import contextlib
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "groth16_proofs_per_s"
+UNIT = "proofs/s"
+# algorithmic Fp multiplications per MSM point (bucket accumulation with the
+# reference's 16-window, 7M+4S mixed-add decomposition) and IMAD-class ops per
+# Fp multiplication (8x8 limb products lo+hi for a*b and m*p, plus m)
+FP_MULTS_PER_POINT = {"accum_g1": 176.0, "accum_g2": 528.0}
+IMAD_PER_FP_MULT = 264.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    p.add_argument("--log-domain", type=int, default=20)
+    p.add_argument("--witness", choices=["uniform", "circom"], default="uniform")
+    p.add_argument("--e2e-steps", type=int, default=0, help="default: min(steps, 5)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workdir", default=os.environ.get("ZK_BENCH_DIR", "/tmp/zyklop_bench"))
+    return p.parse_args()
+
+
+# ------------------------------------------------------------ distributed
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            self.pg.barrier(device_ids=[self.local])
+            torch.cuda.synchronize()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([float(x)], device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "power_w_max": max(power) if power else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+@contextlib.contextmanager
+def silenced():
+    """Silence fd 1 / 2 (the reference prover prints progress on both)."""
+    sys.stdout.flush()
+    sys.stderr.flush()
+    saved = os.dup(1), os.dup(2)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    os.dup2(devnull, 2)
+    try:
+        yield
+    finally:
+        os.dup2(saved[0], 1)
+        os.dup2(saved[1], 2)
+        os.close(devnull)
+        os.close(saved[0])
+        os.close(saved[1])
+
+
+# ------------------------------------------------------------- workload
+def circuit_files(args, dist):
+    tag = f"l{args.log_domain}_{args.witness}_s1"
+    d = os.path.join(args.workdir, tag)
+    z, w = os.path.join(d, "circuit.zkey"), os.path.join(d, "witness.wtns")
+    done = os.path.join(d, "ok")
+    if dist.rank == 0 and not os.path.exists(done):
+        os.makedirs(d, exist_ok=True)
+        from zyklop_b200 import api
+        nnz = (2, 2) if args.witness == "uniform" else (1, 4)
+        api.synth_circuit(z, w, args.log_domain, n_public=8, n_private_inputs=8, nnz=nnz,
+                          witness=args.witness, seed=1)
+        open(done, "w").write("ok\n")
+    dist.barrier()
+    return z, w
+
+
+def zkey_bytes(z, sections):
+    data = open(z, "rb").read(12)
+    total = 0
+    with open(z, "rb") as f:
+        f.seek(8)
+        ns = int.from_bytes(f.read(4), "little")
+        for _ in range(ns):
+            t = int.from_bytes(f.read(4), "little")
+            s = int.from_bytes(f.read(8), "little")
+            if t in sections:
+                total += s
+            f.seek(s, 1)
+    return total
+
+
+def config(args, n_vars, domain):
+    return {"workload": f"groth16_prove_2^{args.log_domain}",
+            "constraints": domain - 9, "domain": domain, "n_vars": n_vars, "n_public": 8,
+            "circuit": "seeded synthetic R1CS, 2 nnz per A/B row (config-0 shape)",
+            "witness": args.witness, "proof": "unblinded (reference-compatible)",
+            "l2": "inputs larger than L2: ~0.6 GB of CRS points and matrices read per proof",
+            "parallelism": f"replicas{args.gpus}"}
+
+
+def cpu_baseline(z, w):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle
+    orc = _oracle.load()
+    zb, wb = open(z, "rb").read(), open(w, "rb").read()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    orc.prove(zb, wb, threads=threads)
+    t = time.perf_counter() - t0
+    return {"value": 1.0 / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "one full proof of the same circuit by the CPU oracle (C, OpenMP; "
+                      f"{t:.1f} s)"}
+
+
+# ------------------------------------------------------------------ mine
+def run_mine(args, dist):
+    import torch
+    torch.cuda.set_device(dist.local)
+    from zyklop_b200 import api
+    from zyklop_b200._lib import Profile, check, lib
+    L = lib()
+    z, w = circuit_files(args, dist)
+    ctx = ctypes.c_void_p()
+    check(L.zk_ctx_create(dist.local, ctypes.byref(ctx)))
+    stream = torch.cuda.current_stream()
+    check(L.zk_ctx_set_stream(ctx, ctypes.c_void_p(stream.cuda_stream)))
+    circuit = api.Circuit(z, ctx=ctx)
+    wit = api.read_wtns(w)
+    dwit = api.to_device(wit)
+    n = wit.shape[0]
+    peak = ctypes.c_double()
+    check(L.zk_imad_probe(ctx, ctypes.byref(peak)))
+    proof = np.zeros(32, np.uint64)
+    pp = proof.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+    def step():
+        check(L.zk_prove_device(circuit.handle, api.ptr(dwit), n, None, None, pp))
+
+    for _ in range(args.warmup):
+        step()
+    reference_proof = proof.copy()
+    torch.cuda.synchronize()
+    check(L.zk_ctx_set_profiling(ctx, 1))
+    prof = Profile()
+    check(L.zk_ctx_profile(ctx, ctypes.byref(prof)))  # clear
+    lc0 = ctypes.c_uint64()
+    check(L.zk_launch_count(ctypes.byref(lc0)))
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+    end.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms = dist.max(start.elapsed_time(end))
+    lc1 = ctypes.c_uint64()
+    check(L.zk_launch_count(ctypes.byref(lc1)))
+    check(L.zk_ctx_profile(ctx, ctypes.byref(prof)))
+    check(L.zk_ctx_set_profiling(ctx, 0))
+    assert np.array_equal(proof, reference_proof), "proofs changed between steps"
+    value = args.gpus * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel kind
+    kinds = {k: (prof.ms[i], prof.launches[i], prof.units[i]) for i, k in enumerate(Profile.KINDS)}
+    dom = max(FP_MULTS_PER_POINT, key=lambda k: kinds[k][0])
+    kms, kl, ku = kinds[dom]
+    achieved = ku * FP_MULTS_PER_POINT[dom] * IMAD_PER_FP_MULT / (kms / 1e3) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic_per_point.json")
+    if os.path.exists(tfile):
+        per_point = json.load(open(tfile)).get(dom)
+        if per_point:
+            traffic = per_point * ku / kl
+    roofline = {"bound": "imad", "kernel": f"k_msm_accum0 ({dom})", "achieved": achieved,
+                "peak": peak.value, "unit": "TIOP/s", "frac": achieved / peak.value,
+                "traffic": traffic,
+                "peak_source": "zk_imad_probe (measured carry-chain IMAD throughput)",
+                "avg_launch_ms": kms / kl, "launches": int(kl),
+                "share_of_step": kms / ms}
+    other = {k: {"ms_per_step": v[0] / args.steps, "launches": int(v[1])} for k, v in kinds.items()}
+
+    # e2e through the one-shot host-buffer entry point
+    e2e_steps = args.e2e_steps or min(args.steps, 5)
+    h2d = zkey_bytes(z, {4, 5, 6, 7, 8, 9}) + os.path.getsize(w)
+    W1, W2 = 17, 17
+    d2h = 256 + 4 * 128 * W1 + 256 * W2
+    check(L.zk_groth16_prove_files(ctx, z.encode(), w.encode(), pp))  # warm the page cache
+    assert np.array_equal(proof, reference_proof)
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        check(L.zk_groth16_prove_files(ctx, z.encode(), w.encode(), pp))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = dist.max(e0.elapsed_time(e1))
+    # resident circuit, host witness (the serving path)
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    for _ in range(e2e_steps):
+        check(L.zk_prove(circuit.handle, wit.ctypes.data_as(ctypes.c_void_p), n, None, None, pp))
+    r1.record(stream)
+    torch.cuda.synchronize()
+    rms = dist.max(r0.elapsed_time(r1))
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact Fr/Fp arithmetic)",
+        "data": "synthetic (seeded circuit, CRS and witness)",
+        "config": config(args, circuit.n_vars, circuit.domain),
+        "e2e": {"value": args.gpus * e2e_steps / (ems / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "call": "zk_groth16_prove_files (zkey + wtns files -> proof)"},
+        "e2e_resident": {"value": args.gpus * e2e_steps / (rms / 1e3), "unit": UNIT,
+                         "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": d2h,
+                         "call": "zk_prove (resident circuit, host witness)"},
+        "roofline": roofline,
+        "kernels": other,
+        "clocks": clk,
+        "gpu_launches": int(lc1.value - lc0.value),
+    }
+    circuit.close()
+    check(L.zk_ctx_destroy(ctx))
+    return line, (z, w)
+
+
+# ------------------------------------------------------------- reference
+def run_reference(args, dist):
+    import torch
+    torch.cuda.set_device(dist.local)
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libzkref_prove.so")
+    if not os.path.exists(lib_path):
+        return {"impl": "reference", "unavailable":
+                "reference sm_100a build missing (oracle/_ref; make -C oracle/refbuild)"}
+    z, w = circuit_files(args, dist)
+    L = ctypes.CDLL(lib_path)
+    L.zkref_prove_files.argtypes = [ctypes.c_char_p, ctypes.c_char_p,
+                                    ctypes.POINTER(ctypes.c_uint64)]
+    proof = np.zeros(32, np.uint64)
+    pp = proof.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+    def step():
+        L.zkref_prove_files(z.encode(), w.encode(), pp)
+
+    with silenced():
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    stream = torch.cuda.current_stream()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with silenced():
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms = dist.max(start.elapsed_time(end))
+    value = args.gpus * args.steps / (ms / 1e3)
+    n_vars = int.from_bytes(open(w, "rb").read()[60:64], "little")
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64 limbs (exact Fr/Fp arithmetic)",
+        "data": "synthetic (seeded circuit, CRS and witness)",
+        "config": config(args, n_vars, 1 << args.log_domain),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 8, "kind": "reference",
+                         "sample": "the reference's own sm_100a build (groth16Prove from "
+                                   "zkey/wtns files; GPU kernels + 8 OpenMP host threads), "
+                                   "every step a full proof"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk,
+    }
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        # rank 0 alone runs the reference; other ranks exit without work and
+        # no process group is formed (so nothing waits on them)
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        os.environ["WORLD_SIZE"] = "1"
+        dist = Dist()
+        line = run_reference(args, dist)
+        print(json.dumps(line), flush=True)
+        return
+    dist = Dist()
+    try:
+        line, files = run_mine(args, dist)
+        if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(*files)
+        if dist.rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

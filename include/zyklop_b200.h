@@ -50,6 +50,35 @@ int zk_ctx_create(int device, zk_ctx** out);
 int zk_ctx_destroy(zk_ctx* ctx);
 /* Synchronize the context's stream. */
 int zk_ctx_sync(zk_ctx* ctx);
+/* Use the caller's CUDA stream (a cudaStream_t) as the context stream.  Every
+ * proof on the context starts after the work already queued on that stream
+ * and finishes before work queued after it, so events recorded there bracket
+ * whole proofs.  Only for contexts from zk_ctx_create. */
+int zk_ctx_set_stream(zk_ctx* ctx, void* stream);
+
+/* ---- measurement ----------------------------------------------------------- */
+/* Number of kernels this library has launched in the process so far. */
+int zk_launch_count(uint64_t* out);
+/* Kernel timing: while on, the hot kernels are bracketed by CUDA events on the
+ * stream they run on.  zk_ctx_profile waits for them, returns per-kind totals
+ * (milliseconds, launches, work units) and clears the record.  Kinds: 0 = G1
+ * bucket accumulation (units: MSM points), 1 = G2 bucket accumulation
+ * (points), 2 = NTT passes (elements), 3 = section-4 SpMV (coefficients).
+ * Replaces the reference's env-gated cudaEvent phase timers (ZK_G1_DEBUG,
+ * ZK_G2_DEBUG, ZK_HPIPE_DEBUG: include/msm_g1.cuh:78-227,
+ * include/msm_g2.cuh:118-200, src/groth16.cu:951-1022). */
+#define ZK_PROF_KINDS 4
+typedef struct {
+  double ms[ZK_PROF_KINDS];
+  double launches[ZK_PROF_KINDS];
+  double units[ZK_PROF_KINDS];
+} zk_profile;
+int zk_ctx_set_profiling(zk_ctx* ctx, int on);
+int zk_ctx_profile(zk_ctx* ctx, zk_profile* out);
+/* Measured carry-chain IMAD throughput of the device (mad.lo.cc / madc.hi.cc,
+ * the field multiplication's instruction mix), in 10^12 ops/s: the
+ * denominator of the MSM roofline.  No reference counterpart. */
+int zk_imad_probe(zk_ctx* ctx, double* tiops);
 
 /* ---- field primitives (device pointers, n elements of 4 x u64) ----------- */
 #define ZK_FIELD_FP 0

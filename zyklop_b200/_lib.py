@@ -26,6 +26,11 @@ SIGNATURES = {
     "zk_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "zk_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_ctx_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "zk_ctx_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "zk_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64)]),
+    "zk_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "zk_ctx_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "zk_imad_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
     "zk_field_op": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p, sz]),
     "zk_ntt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int]),
@@ -108,3 +113,9 @@ def check(rc):
 
 def version():
     return lib().zk_version().decode()
+
+
+class Profile(ctypes.Structure):
+    KINDS = ("accum_g1", "accum_g2", "ntt_pass", "spmv")
+    _fields_ = [("ms", ctypes.c_double * 4), ("launches", ctypes.c_double * 4),
+                ("units", ctypes.c_double * 4)]

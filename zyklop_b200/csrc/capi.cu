@@ -94,8 +94,54 @@ int zk_ctx_destroy(zk_ctx* ctx) {
   if (!ctx || ctx->is_default) return ZK_OK;
   use_device(ctx);
   cudaStreamSynchronize(ctx->stream);
-  cudaStreamDestroy(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+  ZK_API_END
+}
+
+int zk_ctx_set_stream(zk_ctx* ctx, void* stream) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(ctx && !ctx->is_default, ZK_EINVAL, "zk_ctx_set_stream: needs a context from zk_ctx_create");
+  enter_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ctx->own_stream) ZK_CUDA(cudaStreamDestroy(ctx->stream));
+  ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+  ctx->own_stream = false;
+  ZK_API_END
+}
+
+int zk_launch_count(uint64_t* out) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(out, ZK_EINVAL, "zk_launch_count: NULL output");
+  *out = launch_count();
+  ZK_API_END
+}
+
+int zk_ctx_set_profiling(zk_ctx* ctx, int on) {
+  ZK_API_BEGIN
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->profiling = on != 0;
+  ZK_API_END
+}
+
+int zk_ctx_profile(zk_ctx* ctx, zk_profile* out) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(out, ZK_EINVAL, "zk_ctx_profile: NULL output");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  static_assert(ZK_PROF_KINDS == kProfKinds, "profile kinds");
+  ctx->prof.collect(out->ms, out->launches, out->units);
+  ZK_API_END
+}
+
+int zk_imad_probe(zk_ctx* ctx, double* tiops) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(tiops, ZK_EINVAL, "zk_imad_probe: NULL output");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  *tiops = imad_probe(ctx->stream);
   ZK_API_END
 }
 
@@ -126,7 +172,7 @@ int zk_field_op(zk_ctx* ctx, int field, int op, uint64_t* d_out, const uint64_t*
       k_field_op<FrCfg><<<g, 256, 0, ctx->stream>>>(op, reinterpret_cast<fr_t*>(d_out),
                                                     reinterpret_cast<const fr_t*>(d_a),
                                                     reinterpret_cast<const fr_t*>(d_b), n);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   ZK_CUDA(cudaStreamSynchronize(ctx->stream));
   ZK_API_END

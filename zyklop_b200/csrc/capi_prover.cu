@@ -12,9 +12,6 @@
 
 using namespace zk;
 
-
-
-
 extern "C" {
 
 int zk_circuit_load_file(zk_ctx* ctx, const char* zkey_path, zk_circuit** out) {
@@ -63,7 +60,7 @@ int zk_prove(zk_circuit* c, const uint64_t* h_witness, size_t n_witness, const u
   ZK_API_BEGIN
   ZK_REQUIRE(c && proof, ZK_EINVAL, "zk_prove: NULL argument");
   ZK_REQUIRE((r == nullptr) == (s == nullptr), ZK_EINVAL, "zk_prove: give both r and s or neither");
-  use_device(c->ctx);
+  enter_ctx(c->ctx);
   std::lock_guard<std::mutex> g(c->ctx->mu);
   prove(c, h_witness, n_witness, false, r, s, proof, nullptr);
   ZK_API_END
@@ -75,7 +72,7 @@ int zk_prove_device(zk_circuit* c, const uint64_t* d_witness, size_t n_witness, 
   ZK_REQUIRE(c && proof, ZK_EINVAL, "zk_prove_device: NULL argument");
   ZK_REQUIRE((r == nullptr) == (s == nullptr), ZK_EINVAL,
              "zk_prove_device: give both r and s or neither");
-  use_device(c->ctx);
+  enter_ctx(c->ctx);
   std::lock_guard<std::mutex> g(c->ctx->mu);
   prove(c, d_witness, n_witness, true, r, s, proof, nullptr);
   ZK_API_END
@@ -85,7 +82,7 @@ int zk_prove_intermediates(zk_circuit* c, const uint64_t* h_witness, size_t n_wi
                            uint64_t* aw, uint64_t* bw, uint64_t* h, uint64_t* proof) {
   ZK_API_BEGIN
   ZK_REQUIRE(c && proof, ZK_EINVAL, "zk_prove_intermediates: NULL argument");
-  use_device(c->ctx);
+  enter_ctx(c->ctx);
   std::lock_guard<std::mutex> g(c->ctx->mu);
   ProveIntermediates dbg;
   dbg.aw = aw;

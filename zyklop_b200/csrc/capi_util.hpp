@@ -29,10 +29,14 @@
 namespace zk {
 const char* last_error();
 
-// ctx or the per-device default context, with its device made current
-inline zk_ctx* resolve_ctx(zk_ctx* ctx) {
-  if (!ctx) return default_ctx();
+// Makes ctx's device current and routes kernel timing to its profiler when
+// profiling is on.
+inline zk_ctx* enter_ctx(zk_ctx* ctx) {
   use_device(ctx);
+  set_current_profiler(ctx->profiling ? &ctx->prof : nullptr);
   return ctx;
 }
+
+// ctx or the per-device default context, entered
+inline zk_ctx* resolve_ctx(zk_ctx* ctx) { return enter_ctx(ctx ? ctx : default_ctx()); }
 }  // namespace zk

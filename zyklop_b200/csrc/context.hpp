@@ -6,6 +6,7 @@
 
 #include "msm.hpp"
 #include "ntt.hpp"
+#include "profile.hpp"
 #include "runtime.hpp"
 
 namespace zk {
@@ -15,7 +16,7 @@ struct ProveWs {
   static constexpr int kStreams = 5;  // 0: witness/SpMV/H/MSM_H, 1: A, 2: B2, 3: C, 4: B1
   bool ready = false;
   cudaStream_t st[kStreams] = {};
-  cudaEvent_t ev_we = nullptr;
+  cudaEvent_t ev_we = nullptr, ev_begin = nullptr;
   cudaEvent_t ev_done[kStreams] = {};
   DeviceBuffer we, aw, bw, cw, h;
   DeviceBuffer msm[kStreams];
@@ -36,6 +37,9 @@ struct zk_ctx {
   zk::MsmConfig msm_cfg[2];
   zk::ProveWs ws;
   zk::Stager stager;
+  zk::Profiler prof;
+  bool profiling = false;
+  bool own_stream = true;  // false after zk_ctx_set_stream
   bool is_default = false;
 };
 

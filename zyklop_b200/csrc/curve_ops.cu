@@ -74,7 +74,7 @@ void mul_generator(int group, const uint64_t* scalars, size_t n, uint64_t* px, u
   else
     k_mul_gen<fp2_t><<<g, 128, 0, st>>>(scalars, n, reinterpret_cast<fp2_t*>(px),
                                         reinterpret_cast<fp2_t*>(py));
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
 }
 
 }  // namespace zk

@@ -10,6 +10,7 @@
 #include "curve.cuh"
 #include "host_field.hpp"
 #include "msm.hpp"
+#include "profile.hpp"
 #include "scan.cuh"
 
 namespace zk {
@@ -455,14 +456,14 @@ int msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* 
     const int th = 256;
     const unsigned g = (unsigned)((n + th - 1) / th);
     k_msm_hist<<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   scan::exclusive(L.counts, L.cursor, s.entries, L.tiles, st);
   if (n) {
     const int th = 256;
     const unsigned g = (unsigned)((n + th - 1) / th);
     k_msm_scatter<<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   const uint32_t* total_p = L.counts + (s.entries - 1);
   const F* fx = reinterpret_cast<const F*>(pts.x);
@@ -470,23 +471,25 @@ int msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* 
   // level 0
   {
     uint32_t* ok = s.levels > 1 ? L.pkey[1] : nullptr;
+    ProfScope prof(g2 ? kProfAccumG2 : kProfAccumG1, (double)n, st);
     k_msm_accum0<F><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
         L.skey, L.sval, total_p, fx, fy, pts.stride, s.k0, L.buckets, ok, L.ppt[1]);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   for (int l = 1; l < s.levels; l++) {
     const int in = l & 1, out = in ^ 1;
     uint32_t* ok = (l + 1 < s.levels) ? L.pkey[out] : nullptr;
     k_msm_accumN<F><<<(unsigned)s.lvl_blocks[l], seg_threads<F>(), 0, st>>>(
         L.pkey[in], L.ppt[in], s.lvl_records[l], s.k1, L.buckets, ok, L.ppt[out]);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   {
     const size_t tot = (size_t)s.W * s.J;
     k_msm_bucket_reduce<F><<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(L.buckets, s.c, s.W, s.B,
                                                                            s.chunk, s.J, L.contrib);
+    ZK_LAUNCHED();
     k_msm_window_reduce<F><<<s.W, 128, 0, st>>>(L.contrib, s.J, L.windows);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   *d_windows = L.windows;
   *c_out = s.c;

@@ -10,6 +10,7 @@
 #include "field.cuh"
 #include "host_field.hpp"
 #include "ntt.hpp"
+#include "profile.hpp"
 
 namespace zk {
 namespace {
@@ -220,11 +221,12 @@ void run_pass(bool dit, const PassArgs& args, int count, const fr_t* tw, int tw_
   const size_t blocks = groups >> log_g;
   const size_t smem = (size_t)8 * 4 * (size_t(1) << (k + log_g));
   dim3 grid((unsigned)blocks, count);
+  ProfScope prof(kProfNttPass, (double)count * (double)(size_t(1) << L), st);
   if (dit)
     k_ntt_pass<true><<<grid, kPassThreads, smem, st>>>(args, tw, tw_shift, L, lo, k, log_g);
   else
     k_ntt_pass<false><<<grid, kPassThreads, smem, st>>>(args, tw, tw_shift, L, lo, k, log_g);
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
 }
 
 // all DIF passes (high bit ranges first); first pass may be out of place
@@ -275,7 +277,7 @@ void NttTables::ensure(int log_n, cudaStream_t st) {
     k_tw_fill<<<blocks_for(half), 256, 0, st>>>(out, reinterpret_cast<const fr_t*>(base),
                                                 reinterpret_cast<const fr_t*>(base + nhi * 32),
                                                 lo_bits, half);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   ZK_CUDA(cudaStreamSynchronize(st));
   lmax = lm;
@@ -297,7 +299,7 @@ void ntt_inplace(NttTables& tw, uint64_t* a, int log_n, bool inverse, void* scra
   fr_t factor{};
   if (inverse) factor = to_dev(Fr::from_u64(n).inv());
   k_bitrev<<<blocks_for(n), 256, 0, st>>>(s, x, log_n, inverse, factor);
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
 }
 
 void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, uint64_t* h,
@@ -310,30 +312,30 @@ void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, u
   fr_t* B = reinterpret_cast<fr_t*>(bw);
   fr_t* C = reinterpret_cast<fr_t*>(cw);
   k_pointwise_mul<<<blocks_for(n), 256, 0, st>>>(A, B, C, n);
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
   PassArgs abc{{A, B, C}, {A, B, C}};
   dif(abc, abc, 3, tw.inv.as<fr_t>(), shift, log_n, st);
   const Fr ninv = Fr::from_u64(n).inv();
   const Fr c_odd = ninv * host_root(log_n + 1);
   k_coset_scale<<<dim3(blocks_for(n), 3), 256, 0, st>>>(abc, tw.fwd.as<fr_t>(), shift, log_n,
                                                         to_dev(ninv), to_dev(c_odd));
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
   dit(abc, 3, tw.fwd.as<fr_t>(), shift, log_n, st);
   k_h_final<<<blocks_for(n), 256, 0, st>>>(A, B, C, reinterpret_cast<fr_t*>(h), n);
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
 }
 
 void fr_encode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t st) {
   if (!n) return;
   k_fr_encode<<<blocks_for(n), 256, 0, st>>>(reinterpret_cast<const fr_t*>(in),
                                              reinterpret_cast<fr_t*>(out), n);
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
 }
 void fr_decode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t st) {
   if (!n) return;
   k_fr_decode<<<blocks_for(n), 256, 0, st>>>(reinterpret_cast<const fr_t*>(in),
                                              reinterpret_cast<fr_t*>(out), n);
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
 }
 
 }  // namespace zk

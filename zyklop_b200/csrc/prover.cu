@@ -8,6 +8,7 @@
 #include "field.cuh"
 #include "host_field.hpp"
 #include "msm.hpp"
+#include "profile.hpp"
 #include "prover.hpp"
 #include "scan.cuh"
 
@@ -112,6 +113,7 @@ void ProveWs::init() {
     ZK_CUDA(cudaEventCreateWithFlags(&ev_done[i], cudaEventDisableTiming));
   }
   ZK_CUDA(cudaEventCreateWithFlags(&ev_we, cudaEventDisableTiming));
+  ZK_CUDA(cudaEventCreateWithFlags(&ev_begin, cudaEventDisableTiming));
   ready = true;
 }
 
@@ -123,6 +125,7 @@ ProveWs::~ProveWs() {
     cudaEventDestroy(ev_done[i]);
   }
   cudaEventDestroy(ev_we);
+  cudaEventDestroy(ev_begin);
 }
 
 zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
@@ -190,7 +193,7 @@ zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
   if (nnz) {
     k_coef_count<<<blocks(nnz, 256), 256, 0, st>>>(raw.as<uint32_t>(), (uint32_t)nnz, (uint32_t)n,
                                                   c->m1, cnt[0], cnt[1], bad);
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   for (int m = 0; m < 2; m++) scan::exclusive(cnt[m], cur[m], n + 1, tl[m], st);
   if (nnz) {
@@ -198,7 +201,7 @@ zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
         raw.as<uint32_t>(), (uint32_t)nnz, (uint32_t)n, c->m1, cur[0], cur[1],
         c->sig[0].as<uint32_t>(), c->sig[1].as<uint32_t>(), c->val[0].as<uint32_t>(),
         c->val[1].as<uint32_t>());
-    ZK_CHECK_LAUNCH();
+    ZK_LAUNCHED();
   }
   for (int m = 0; m < 2; m++)
     ZK_CUDA(cudaMemcpyAsync(c->row[m].ptr, cnt[m], 4 * (n + 1), cudaMemcpyDeviceToDevice, st));
@@ -238,6 +241,11 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
       ws.msm[i].ensure(need[i]);
     }
 
+  // the proof starts after prior work on the context stream and ends before
+  // later work on it, so callers can bracket it with events on that stream
+  ZK_CUDA(cudaEventRecord(ws.ev_begin, ctx->stream));
+  for (int i = 0; i < ProveWs::kStreams; i++) ZK_CUDA(cudaStreamWaitEvent(ws.st[i], ws.ev_begin, 0));
+
   // 1. witness: we = [1 || w_0 .. w_{m1-1}] (src/groth16.cu:1316-1326)
   cudaStream_t s0 = ws.st[0];
   uint64_t* we = ws.we.as<uint64_t>();
@@ -276,8 +284,12 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   }
   sa.out[0] = ws.aw.as<fr_t>();
   sa.out[1] = ws.bw.as<fr_t>();
+  {
+  ProfScope prof(kProfSpmv, (double)c->n_coefs, s0);
   k_spmv<<<dim3(blocks(n, 256), 2), 256, 0, s0>>>(sa, reinterpret_cast<const fr_t*>(we + 4),
                                                   (uint32_t)n);
+  ZK_LAUNCHED();
+  }
   ZK_CHECK_LAUNCH();
   if (dbg && (dbg->aw || dbg->bw)) {
     if (dbg->aw) ZK_CUDA(cudaMemcpyAsync(dbg->aw, ws.aw.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
@@ -294,6 +306,7 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
 
   // 4. host: combine the window sums, assemble the proof
   const int used = blind ? 5 : 4;
+  for (int i = 0; i < used; i++) ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_done[i], 0));
   for (int i = 0; i < used; i++) ZK_CUDA(cudaEventSynchronize(ws.ev_done[i]));
   uint64_t pa[8], pb[16], pc[8], ph[8], pb1[8];
   msm_g1_combine(ws.win[1].ptr, W[1], C[1], pa);

@@ -35,6 +35,14 @@ struct Error : std::runtime_error {
 
 #define ZK_CHECK_LAUNCH() ZK_CUDA(cudaGetLastError())
 
+void count_launch(int n);
+// after every kernel launch: counts it and surfaces launch errors
+#define ZK_LAUNCHED()            \
+  do {                           \
+    ::zk::count_launch(1);       \
+    ZK_CHECK_LAUNCH();           \
+  } while (0)
+
 #define ZK_REQUIRE(cond, code, msg)                         \
   do {                                                      \
     if (!(cond)) throw ::zk::Error((code), (msg));          \

@@ -97,9 +97,11 @@ inline void exclusive(uint32_t* a, uint32_t* copy, size_t n, uint32_t* tiles, cu
   if (!n) return;
   const size_t nt = tile_count(n);
   k_tiles<<<(unsigned)nt, 1024, 0, st>>>(a, n, tiles);
+  ZK_LAUNCHED();
   k_top<<<1, 1024, 0, st>>>(tiles, nt);
+  ZK_LAUNCHED();
   k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, copy, n, tiles);
-  ZK_CHECK_LAUNCH();
+  ZK_LAUNCHED();
 }
 
 }  // namespace
