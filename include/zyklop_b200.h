@@ -126,6 +126,20 @@ int zk_msm_g1(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uin
 int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
               size_t n, uint64_t* h_out, int* is_inf);
 
+/* G1 MSM that allocates nothing, for callers that cannot call cudaMalloc (a
+ * plugin inside a host application that has given all device memory to its
+ * own pool allocator, or a latency-critical loop that cannot take
+ * cudaMalloc's implicit device synchronization).  Same inputs and result as
+ * zk_msm_g1, on the caller's `stream` (a cudaStream_t; NULL = default
+ * stream); blocks until the result is on the host.  Its scratch is a fixed
+ * 24 MiB __device__ array, so n is limited to 65536 points (larger n returns
+ * ZK_EINVAL).  The first call on each device looks up that array's address
+ * once; make it before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race, so serialize them.  No counterpart in the
+ * reference. */
+int zk_msm_g1_noalloc(const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
+                      size_t n, uint64_t* h_out, int* is_inf, void* stream);
+
 /* Pippenger parameters for subsequent MSMs on this context (group 1 or 2):
  * window bits c (0 = automatic), records per thread k0 / k1, buckets per
  * thread in the bucket reduction.  Replaces the reference's compile-time

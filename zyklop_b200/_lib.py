@@ -40,6 +40,8 @@ SIGNATURES = {
                                  sz, u64p, c_int_p]),
     "zk_msm_g2": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                  sz, u64p, c_int_p]),
+    "zk_msm_g1_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, sz,
+                                         u64p, c_int_p, ctypes.c_void_p]),
     "zk_msm_set_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int]),
     "zk_msm_scratch_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, sz,

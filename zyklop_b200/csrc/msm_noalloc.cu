@@ -1,0 +1,100 @@
+// zk_msm_g1_noalloc: the G1 MSM for callers that cannot allocate device
+// memory.
+//
+// Some callers cannot call cudaMalloc: a plugin loaded into a host
+// application that has already handed all of the device's memory to its own
+// pool allocator, or a latency-critical loop where cudaMalloc's implicit
+// device-wide synchronization is not acceptable.  This entry point runs the
+// same MSM kernels as zk_msm_g1, but its scratch lives in a file-scope
+// __device__ array of fixed size instead of a context arena, and it takes the
+// caller's stream instead of a context, so it needs no allocation of its own.
+//
+// Limits and rules:
+//   * at most kNoAllocMaxPoints = 2^16 points per call (the scratch array is
+//     24 MiB and is held by every GPU that loads the library until exit);
+//   * the first call on a device looks up the array's device address with
+//     cudaGetSymbolAddress (once per device, with that device current); make
+//     that first call before any stream capture;
+//   * every call shares the one array: calls whose work overlaps on the GPU
+//     (different streams, or different host threads) race and give wrong
+//     results, so serialize them;
+//   * the array keeps the previous call's contents; the kernels clear what
+//     must start at zero (bucket counts and bucket sums) at the start of
+//     every call.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <mutex>
+
+#include "capi_util.hpp"
+#include "msm.hpp"
+#include "profile.hpp"
+#include "runtime.hpp"
+
+namespace {
+
+constexpr size_t kNoAllocMaxPoints = size_t(1) << 16;
+constexpr size_t kNoAllocScratchBytes = size_t(24) << 20;
+constexpr int kMaxWindows = 64;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// host-side: the array's device address on each device (null until set up)
+void* g_noalloc_addr[kMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+int fail(int code, const char* msg) {
+  zk::set_last_error(code, msg);
+  return code;
+}
+
+}  // namespace
+
+extern "C" int zk_msm_g1_noalloc(const uint64_t* d_px, const uint64_t* d_py,
+                                 const uint64_t* d_scalars, size_t n, uint64_t* h_out,
+                                 int* is_inf, void* stream) {
+  if (!h_out) return fail(ZK_EINVAL, "zk_msm_g1_noalloc: NULL output");
+  if (n && !(d_px && d_py && d_scalars)) return fail(ZK_EINVAL, "zk_msm_g1_noalloc: NULL input");
+  if (n > kNoAllocMaxPoints) {
+    char msg[160];
+    snprintf(msg, sizeof(msg),
+             "zk_msm_g1_noalloc: %zu points exceed the maximum of %zu (fixed scratch of %zu MiB); "
+             "use zk_msm_g1 for larger MSMs",
+             n, kNoAllocMaxPoints, kNoAllocScratchBytes >> 20);
+    return fail(ZK_EINVAL, msg);
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(ZK_ECUDA, cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return fail(ZK_ENOTSUP, "zk_msm_g1_noalloc: device index too large");
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      // once per device, with that device current (it is: cudaGetDevice above)
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) return fail(ZK_ECUDA, "zk_msm_g1_noalloc: cudaGetSymbolAddress failed");
+      g_noalloc_addr[dev] = p;
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  ZK_API_BEGIN
+  zk::set_current_profiler(nullptr);  // no event recording (it would create events)
+  const zk::MsmConfig cfg;
+  ZK_REQUIRE(zk::msm_scratch_bytes(n, false, cfg) <= kNoAllocScratchBytes, ZK_EINTERNAL,
+             "zk_msm_g1_noalloc: scratch layout exceeds the fixed array");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const void* d_windows = nullptr;
+  int c = 0;
+  const int W = zk::msm_g1_enqueue(zk::points_soa(d_px, d_py), d_scalars, n, scratch,
+                                   kNoAllocScratchBytes, cfg, st, &d_windows, &c);
+  ZK_REQUIRE(W <= kMaxWindows, ZK_EINTERNAL, "zk_msm_g1_noalloc: too many windows");
+  alignas(16) unsigned char h_windows[kMaxWindows * 128];
+  ZK_CUDA(cudaMemcpyAsync(h_windows, d_windows, (size_t)W * 128, cudaMemcpyDeviceToHost, st));
+  ZK_CUDA(cudaStreamSynchronize(st));
+  const bool inf = zk::msm_g1_combine(h_windows, W, c, h_out);
+  if (is_inf) *is_inf = inf ? 1 : 0;
+  ZK_API_END
+}
