@@ -140,9 +140,23 @@ int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uin
 int zk_msm_g1_noalloc(const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
                       size_t n, uint64_t* h_out, int* is_inf, void* stream);
 
+/* Fixed-base MSM: precompute once for a resident set of n points of prime
+ * order r (group 1: n x 4 u64 coordinates, group 2: n x 8), then run MSMs
+ * against it with any scalars (reduced mod r).  c = 0 picks the window size.
+ * The table holds (254/c + 1) multiples per point.  zk_msm_table_run takes up
+ * to n scalars (missing ones count as zero) and returns the same affine
+ * result as zk_msm_g1 / zk_msm_g2 on those points.  No reference
+ * counterpart (the reference recomputes every window from the bases). */
+typedef struct zk_msm_table zk_msm_table;
+int zk_msm_table_create(zk_ctx* ctx, int group, const uint64_t* d_px, const uint64_t* d_py,
+                        size_t n, int c, zk_msm_table** out);
+int zk_msm_table_run(zk_msm_table* t, const uint64_t* d_scalars, size_t n, uint64_t* h_out,
+                     int* is_inf);
+int zk_msm_table_free(zk_msm_table* t);
+
 /* Pippenger parameters for subsequent MSMs on this context (group 1 or 2):
- * window bits c (0 = automatic), records per thread k0 / k1, buckets per
- * thread in the bucket reduction.  Replaces the reference's compile-time
+ * window bits c (0 = automatic), records per thread k0 / k1, and the fan-in
+ * `chunk` (a power of two) of each bucket-reduction level.  Replaces the reference's compile-time
  * MSM_G1_C_BITS / C_BITS and ZK_G1_* / ZK_G2_* environment knobs
  * (include/msm_g1.cuh:45-117, include/msm_g2.cuh:39-116). */
 int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk);
@@ -161,6 +175,16 @@ int zk_circuit_load_file(zk_ctx* ctx, const char* zkey_path, zk_circuit** out);
 int zk_circuit_load_mem(zk_ctx* ctx, const uint8_t* zkey, size_t len, zk_circuit** out);
 int zk_circuit_free(zk_circuit* c);
 int zk_circuit_info(const zk_circuit* c, uint32_t* n_vars, uint32_t* n_public, uint32_t* domain);
+
+/* Builds fixed-base tables for the circuit's point sets: for each point P
+ * and window w < 254/c + 1 the multiple 2^(c w) P, kept resident (W times the
+ * points' memory).  Later proofs then sort every (point, window) digit into
+ * one shared bucket set: one bucket reduction per MSM instead of one per
+ * window and no doubling chain, with larger windows (fewer additions).
+ * c_g1 / c_g2: window bits (0 = default for the size).  Proofs are
+ * unchanged bit for bit.  The CRS-residency format of SURVEY 8(f) row 2;
+ * the reference has no counterpart. */
+int zk_circuit_precompute(zk_circuit* c, int c_g1, int c_g2);
 
 /* Proves with a witness of n_witness >= nVars canonical Fr values (wtns
  * section 2 layout).  r, s: canonical Fr blinding scalars, or both NULL for

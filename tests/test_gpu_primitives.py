@@ -319,3 +319,30 @@ def test_mul_generator_vs_oracle(api, oracle, group):
     for i, k in enumerate(ks):
         exp = oracle.g1_mul(g, k) if group == 1 else oracle.g2_mul(g, k)
         assert np.array_equal(np.concatenate([px[i], py[i]]), exp), (group, i)
+
+
+@pytest.mark.parametrize("group,n,c", [(1, 1, 0), (1, 100, 8), (1, 5000, 0), (1, 1 << 16, 0),
+                                       (1, 3000, 13), (2, 50, 0), (2, 3000, 0), (2, 2048, 11)])
+def test_fixed_base_table_matches_windowed(api, oracle, group, n, c):
+    """zk_msm_table (precomputed 2^(cw) multiples, one shared bucket set) gives
+    the same affine point as the windowed MSM, including for scalars >= r
+    (reduced mod r against points of order r) and for partial scalar vectors."""
+    rng = np.random.default_rng(group * 1000 + n)
+    base = scalars(rng, n)
+    px, py = api.mul_generator(group, base)
+    sc = scalars(rng, n)
+    if n >= 4:
+        over = int.from_bytes(rng.bytes(32), "little") % R
+        sc[1] = limbs(over + R)        # >= r
+        sc[2] = limbs(2**256 - 1)      # maximal 256-bit integer
+        sc[3] = 0
+    t = api.MsmTable(group, px, py, c=c)
+    got, ginf = t.run(sc)
+    want, winf = (api.msm_g1 if group == 1 else api.msm_g2)(px, py, sc)
+    assert ginf == winf and np.array_equal(got, want)
+    if n > 10:
+        k = n // 2  # fewer scalars than table points: the rest count as zero
+        got, _ = t.run(sc[:k])
+        want, _ = (api.msm_g1 if group == 1 else api.msm_g2)(px[:k], py[:k], sc[:k])
+        assert np.array_equal(got, want)
+    t.close()

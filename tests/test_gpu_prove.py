@@ -85,6 +85,23 @@ def test_prove_matches_oracle(api, oracle, files, name):
     assert np.array_equal(mine, oracle.prove(blob(z), blob(w)))
 
 
+@pytest.mark.parametrize("name", ["u10", "c10", "u16"])
+def test_precomputed_circuit_gives_identical_proofs(api, oracle, files, name):
+    """Fixed-base tables change how the MSMs run, not what they compute."""
+    z, w = files[name]
+    c = api.Circuit(z)
+    wit = api.read_wtns(w)
+    plain = c.prove(wit)
+    c.precompute()
+    assert np.array_equal(c.prove(wit), plain)
+    r, s = 0x1234567890ABCDEF, 0xFEDCBA0987654321
+    blinded = c.prove(wit, r=r, s=s)
+    assert np.array_equal(blinded, oracle.prove(blob(z), blob(w), r=r, s=s))
+    c2 = api.Circuit(z)
+    c2.precompute(c_g1=11, c_g2=9)
+    assert np.array_equal(c2.prove(wit), plain)
+
+
 @pytest.mark.parametrize("name", ["u10", "c10"])
 def test_intermediates_match_oracle(api, oracle, files, name):
     z, w = files[name]

@@ -42,6 +42,12 @@ SIGNATURES = {
                                  sz, u64p, c_int_p]),
     "zk_msm_g1_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, sz,
                                          u64p, c_int_p, ctypes.c_void_p]),
+    "zk_msm_table_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                           ctypes.c_void_p, sz, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "zk_msm_table_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz, u64p, c_int_p]),
+    "zk_msm_table_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "zk_circuit_precompute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "zk_msm_set_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int]),
     "zk_msm_scratch_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, sz,

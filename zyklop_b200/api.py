@@ -147,6 +147,9 @@ class Circuit:
         check(lib().zk_circuit_info(h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         self.n_vars, self.n_public, self.domain = a.value, b.value, c.value
 
+    def precompute(self, c_g1=0, c_g2=0):
+        check(lib().zk_circuit_precompute(self.handle, c_g1, c_g2))
+
     def prove(self, witness, r=None, s=None):
         w = np.ascontiguousarray(witness, dtype=np.uint64).reshape(-1, 4)
         proof = np.zeros(32, dtype=np.uint64)
@@ -228,3 +231,36 @@ def public_json(wtns_path, n_public):
     buf = ctypes.create_string_buffer(size)
     check(lib().zk_public_json(str(wtns_path).encode(), n_public, buf, size))
     return buf.value.decode()
+
+
+class MsmTable:
+    """Fixed-base MSM table (zk_msm_table_create / zk_msm_table_run)."""
+
+    def __init__(self, group, px, py, c=0, ctx=None):
+        self.group = group
+        self.dx, self.dy = to_device(px), to_device(py)
+        h = ctypes.c_void_p()
+        n = np.asarray(px).shape[0]
+        check(lib().zk_msm_table_create(ctx, group, ptr(self.dx), ptr(self.dy), n, c,
+                                        ctypes.byref(h)))
+        self.handle = h
+
+    def run(self, scalars):
+        sc = np.ascontiguousarray(scalars, dtype=np.uint64).reshape(-1, 4)
+        ds = to_device(sc)
+        out = np.zeros(8 if self.group == 1 else 16, dtype=np.uint64)
+        inf = ctypes.c_int(0)
+        check(lib().zk_msm_table_run(self.handle, ptr(ds), sc.shape[0],
+                                     out.ctypes.data_as(_u64p), ctypes.byref(inf)))
+        return out, bool(inf.value)
+
+    def close(self):
+        if self.handle:
+            lib().zk_msm_table_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "capi_util.hpp"
+#include "msm.hpp"
 #include "prover.hpp"
 #include "serialize.hpp"
 
@@ -52,6 +53,81 @@ int zk_circuit_info(const zk_circuit* c, uint32_t* n_vars, uint32_t* n_public, u
   if (n_vars) *n_vars = c->m1;
   if (n_public) *n_public = c->l;
   if (domain) *domain = c->n;
+  ZK_API_END
+}
+
+int zk_circuit_precompute(zk_circuit* c, int c_g1, int c_g2) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(c, ZK_EINVAL, "zk_circuit_precompute: NULL circuit");
+  enter_ctx(c->ctx);
+  std::lock_guard<std::mutex> g(c->ctx->mu);
+  circuit_precompute(c, c_g1, c_g2);
+  ZK_API_END
+}
+
+int zk_msm_table_create(zk_ctx* ctx, int group, const uint64_t* d_px, const uint64_t* d_py,
+                        size_t n, int c, zk_msm_table** out) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(out, ZK_EINVAL, "zk_msm_table_create: NULL output");
+  *out = nullptr;
+  ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_msm_table_create: group must be 1 or 2");
+  ZK_REQUIRE(n == 0 || (d_px && d_py), ZK_EINVAL, "zk_msm_table_create: NULL points");
+  ZK_REQUIRE(n < (size_t(1) << 27), ZK_EINVAL, "zk_msm_table_create: too many points");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  std::unique_ptr<zk_msm_table> t(new zk_msm_table());
+  t->ctx = ctx;
+  t->group = group;
+  t->n = n;
+  t->c = c ? c : msm_fixed_default_c(n, group == 2);
+  ZK_REQUIRE(t->c >= 4 && t->c <= 22, ZK_EINVAL, "zk_msm_table_create: c must be 0 or 4..22");
+  t->table.ensure(msm_table_bytes(n ? n : 1, group == 2, t->c));
+  msm_precompute(group == 2, points_soa(d_px, d_py), n, t->c, t->table.ptr, ctx->stream);
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  *out = t.release();
+  ZK_API_END
+}
+
+int zk_msm_table_run(zk_msm_table* t, const uint64_t* d_scalars, size_t n, uint64_t* h_out,
+                     int* is_inf) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(t && h_out, ZK_EINVAL, "zk_msm_table_run: NULL argument");
+  ZK_REQUIRE(n <= t->n, ZK_EINVAL, "zk_msm_table_run: more scalars than table points");
+  ZK_REQUIRE(n == 0 || d_scalars, ZK_EINVAL, "zk_msm_table_run: NULL scalars");
+  zk_ctx* ctx = enter_ctx(t->ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  const bool g2 = t->group == 2;
+  const MsmConfig& cfg = ctx->msm_cfg[g2 ? 1 : 0];
+  // the table's records are laid out for t->n points: run over all of them
+  // with zero scalars past n (a prefix of the table is not a table)
+  const size_t cnt = t->n;
+  DeviceBuffer sc;
+  const uint64_t* scal = d_scalars;
+  if (n < cnt) {
+    sc.ensure(32 * cnt);
+    ZK_CUDA(cudaMemsetAsync(sc.ptr, 0, 32 * cnt, ctx->stream));
+    if (n) ZK_CUDA(cudaMemcpyAsync(sc.ptr, d_scalars, 32 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    scal = sc.as<uint64_t>();
+  }
+  ctx->msm_scratch.ensure(msm_scratch_bytes_fixed(cnt, g2, t->c, cfg));
+  const void* dw;
+  int cc;
+  const int W = msm_enqueue_fixed(g2, t->table.ptr, scal, cnt, t->c, ctx->msm_scratch.ptr,
+                                  ctx->msm_scratch.cap, cfg, ctx->stream, &dw, &cc);
+  uint8_t h[512];
+  ZK_CUDA(cudaMemcpyAsync(h, dw, (size_t)W * (g2 ? 256 : 128), cudaMemcpyDeviceToHost, ctx->stream));
+  ZK_CUDA(cudaStreamSynchronize(ctx->stream));
+  const bool inf = g2 ? msm_g2_combine(h, W, cc, h_out) : msm_g1_combine(h, W, cc, h_out);
+  if (is_inf) *is_inf = inf ? 1 : 0;
+  ZK_API_END
+}
+
+int zk_msm_table_free(zk_msm_table* t) {
+  ZK_API_BEGIN
+  if (!t) return ZK_OK;
+  enter_ctx(t->ctx);
+  std::lock_guard<std::mutex> g(t->ctx->mu);
+  delete t;
   ZK_API_END
 }
 

@@ -22,25 +22,31 @@ constexpr uint32_t kNeg = 0x80000000u;
 // ------------------------------------------------------------------ shape
 struct Shape {
   size_t n;
-  int c, W;
-  uint32_t B;            // buckets per window (2^(c-1))
+  int c, W;              // window bits, scalar windows
+  int Wk;                // bucket sets: W, or 1 when windows share buckets (fixed bases)
+  bool fixed;            // points carry precomputed 2^(c w) multiples (table of W*n records)
+  uint32_t B;            // buckets per set (2^(c-1))
   size_t entries;        // W*B + 1 scan entries (last = total)
   size_t records;        // W*n upper bound on sorted records
   int k0, k1, chunk;
   int levels;            // segmented-reduction levels (>= 1)
   size_t lvl_records[24];
   size_t lvl_blocks[24];
-  size_t J;              // bucket-reduction chunks per window
+  size_t J;              // bucket-reduction level-1 chunks per window
 };
 
-Shape make_shape(size_t n, bool g2, const MsmConfig& cfg) {
+Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false) {
   const int seg_t = g2 ? 64 : 128;
   Shape s{};
   s.n = n;
   s.c = cfg.c > 0 ? cfg.c : msm_default_c(n, g2);
-  s.W = 256 / s.c + 1;  // top window holds < c bits, so no carry leaves it
+  // the top window holds < c bits, so no carry leaves it; fixed-base MSMs
+  // reduce scalars mod r first (254 bits)
+  s.fixed = fixed;
+  s.W = (fixed ? 254 : 256) / s.c + 1;
+  s.Wk = fixed ? 1 : s.W;
   s.B = 1u << (s.c - 1);
-  s.entries = (size_t)s.W * s.B + 1;
+  s.entries = (size_t)s.Wk * s.B + 1;
   s.records = std::max<size_t>((size_t)s.W * n, 1);
   s.k0 = cfg.k0;
   s.k1 = cfg.k1;
@@ -72,8 +78,9 @@ struct Layout {
   xyzz<F>* buckets;   // W*B
   uint32_t* pkey[2];  // ping-pong partial records
   xyzz<F>* ppt[2];
-  xyzz<F>* contrib;   // W*J
-  xyzz<F>* windows;   // W
+  xyzz<F>* rrun[2];   // bucket-reduction (run, acc) pairs, ping-pong
+  xyzz<F>* racc[2];
+  xyzz<F>* windows;   // W window sums (points into racc)
   size_t bytes;
 };
 
@@ -86,15 +93,19 @@ Layout<F> carve(void* base, const Shape& s) {
   L.tiles = cv.take<uint32_t>(scan::tile_count(s.entries) + 1);
   L.skey = cv.take<uint32_t>(s.records);
   L.sval = cv.take<uint32_t>(s.records);
-  L.buckets = cv.take<xyzz<F>>((size_t)s.W * s.B);
+  L.buckets = cv.take<xyzz<F>>((size_t)s.Wk * s.B);
   size_t pmax[2] = {1, 1};
   for (int l = 1; l < s.levels; l++) pmax[l & 1] = std::max(pmax[l & 1], s.lvl_records[l]);
   for (int i = 0; i < 2; i++) {
     L.pkey[i] = cv.take<uint32_t>(pmax[i]);
     L.ppt[i] = cv.take<xyzz<F>>(pmax[i]);
   }
-  L.contrib = cv.take<xyzz<F>>((size_t)s.W * s.J);
-  L.windows = cv.take<xyzz<F>>((size_t)s.W);
+  const size_t j2 = (s.J + s.chunk - 1) / s.chunk;
+  L.rrun[0] = cv.take<xyzz<F>>((size_t)s.Wk * s.J);
+  L.racc[0] = cv.take<xyzz<F>>((size_t)s.Wk * s.J);
+  L.rrun[1] = cv.take<xyzz<F>>((size_t)s.Wk * j2);
+  L.racc[1] = cv.take<xyzz<F>>((size_t)s.Wk * j2);
+  L.windows = nullptr;
   L.bytes = cv.off + 256;
   return L;
 }
@@ -135,23 +146,54 @@ __device__ __forceinline__ uint32_t next_digit(uint32_t s[8], int c, uint32_t B,
   return mag ? (uint32_t)w * B + (mag - 1) : kInvalid;
 }
 
+// k mod r for a 256-bit k (at most 5 subtractions of r < 2^254): fixed-base
+// tables hold multiples of points of order r, so k and k mod r give the same
+// sum, and the reduced scalar fits the tables' 254-bit window range.
+__device__ __forceinline__ void reduce_mod_r(uint32_t s[8]) {
+  for (int it = 0; it < 5; it++) {
+    uint32_t d[8], bw;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]),
+          "=r"(d[7]), "=r"(bw)
+        : "r"(s[0]), "r"(s[1]), "r"(s[2]), "r"(s[3]), "r"(s[4]), "r"(s[5]), "r"(s[6]), "r"(s[7]),
+          "n"(FrCfg::P0), "n"(FrCfg::P1), "n"(FrCfg::P2), "n"(FrCfg::P3), "n"(FrCfg::P4),
+          "n"(FrCfg::P5), "n"(FrCfg::P6), "n"(FrCfg::P7));
+    if (bw) return;  // s < r
+#pragma unroll
+    for (int q = 0; q < 8; q++) s[q] = d[q];
+  }
+}
+
+// kFixed: all windows share one bucket set, and the record value names the
+// table entry (window w of point i: w * n + i) instead of the point.
+template <bool kFixed>
 __global__ void k_msm_hist(const uint64_t* __restrict__ sc, size_t n, int c, int W, uint32_t B,
                            uint32_t* __restrict__ counts) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i < n;
   uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (active) load_scalar(sc, i, s);
+  if (kFixed) reduce_mod_r(s);
   const int lane = threadIdx.x & 31;
   uint32_t carry = 0;
   for (int w = 0; w < W; w++) {
     bool neg;
-    uint32_t key = next_digit(s, c, B, w, carry, neg);
+    uint32_t key = next_digit(s, c, B, kFixed ? 0 : w, carry, neg);
     if (!active) key = kInvalid;
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     if (key != kInvalid && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
   }
 }
 
+template <bool kFixed>
 __global__ void k_msm_scatter(const uint64_t* __restrict__ sc, size_t n, int c, int W, uint32_t B,
                               uint32_t* __restrict__ cursor, uint32_t* __restrict__ skey,
                               uint32_t* __restrict__ sval) {
@@ -159,12 +201,13 @@ __global__ void k_msm_scatter(const uint64_t* __restrict__ sc, size_t n, int c, 
   const bool active = i < n;
   uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (active) load_scalar(sc, i, s);
+  if (kFixed) reduce_mod_r(s);
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   uint32_t carry = 0;
   for (int w = 0; w < W; w++) {
     bool neg;
-    uint32_t key = next_digit(s, c, B, w, carry, neg);
+    uint32_t key = next_digit(s, c, B, kFixed ? 0 : w, carry, neg);
     if (!active) key = kInvalid;
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     const int leader = __ffs(peers) - 1;
@@ -174,7 +217,8 @@ __global__ void k_msm_scatter(const uint64_t* __restrict__ sc, size_t n, int c, 
     if (key != kInvalid) {
       const uint32_t pos = base + __popc(peers & lt);
       skey[pos] = key;
-      sval[pos] = (uint32_t)i | (neg ? kNeg : 0u);
+      const uint32_t idx = kFixed ? (uint32_t)((size_t)w * n + i) : (uint32_t)i;
+      sval[pos] = idx | (neg ? kNeg : 0u);
     }
   }
 }
@@ -380,89 +424,129 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accumN(
 }
 
 // ------------------------------------------------------ bucket reduction
+// Window sums sum_b (b+1) S_b without per-chunk scalar multiplications.
+// Level 1: thread per (window, chunk of L buckets) -> (run, acc) with
+// run = sum S_b and acc = sum (i+1) S_{lo+i} (running sums from the top).
+// Level k > 1: thread per (window, group of G consecutive level-(k-1) pairs,
+// each covering `span` buckets) -> run' = sum run_i and
+// acc' = sum acc_i + span * sum_i i run_i, where sum_i i run_i is again a
+// running sum and span is a power of two (log2(span) doublings).  The last
+// level leaves one pair per window; its acc is the window sum.
 template <class F>
-__device__ __forceinline__ xyzz<F> xyzz_mul_small(const xyzz<F>& p, uint32_t k) {
-  xyzz<F> r = xyzz_inf<F>();
-  if (k == 0) return r;
-  const int top = 31 - __clz(k);
-  r = p;
-  for (int i = top - 1; i >= 0; i--) {
-    r = xyzz_dbl(r);
-    if ((k >> i) & 1) r = xyzz_add(r, p);
-  }
-  return r;
-}
-
-// thread per (window, chunk): sum_{b in chunk} (b+1) S_b
-template <class F>
-__global__ void __launch_bounds__(128) k_msm_bucket_reduce(const xyzz<F>* __restrict__ buckets,
-                                                           int c, int W, uint32_t B, int chunk,
-                                                           size_t J, xyzz<F>* __restrict__ contrib) {
+__global__ void __launch_bounds__(128) k_msm_reduce_l1(const xyzz<F>* __restrict__ buckets, int c,
+                                                       int W, uint32_t B, uint32_t L, uint32_t J,
+                                                       xyzz<F>* __restrict__ run_out,
+                                                       xyzz<F>* __restrict__ acc_out) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (size_t)W * J) return;
   const int w = (int)(t / J);
   const uint32_t j = (uint32_t)(t % J);
   const int nbits = 256 - w * c;
   const uint32_t Bw = nbits >= c ? B : (nbits <= 0 ? 1u : (1u << nbits));
-  const uint32_t lo = j * chunk;
-  xyzz<F> out = xyzz_inf<F>();
+  const uint32_t lo = j * L;
+  xyzz<F> run = xyzz_inf<F>(), acc = xyzz_inf<F>();
   if (lo < Bw) {
-    const uint32_t hi = min(lo + (uint32_t)chunk, Bw);
+    const uint32_t hi = min(lo + L, Bw);
     const xyzz<F>* bw = buckets + (size_t)w * B;
-    xyzz<F> run = xyzz_inf<F>(), acc = xyzz_inf<F>();
     for (uint32_t b = hi; b-- > lo;) {
       run = xyzz_add(run, ld_pod(bw + b));
       acc = xyzz_add(acc, run);
     }
-    // buckets lo..hi-1 hold digits lo+1..hi: add lo * run for the offset
-    out = xyzz_add(acc, xyzz_mul_small(run, lo));
   }
-  st_pod(&contrib[t], out);
+  st_pod(&run_out[t], run);
+  st_pod(&acc_out[t], acc);
 }
 
-// block per window: tree-sum of its chunk contributions
 template <class F>
-__global__ void __launch_bounds__(128) k_msm_window_reduce(const xyzz<F>* __restrict__ contrib,
-                                                           size_t J, xyzz<F>* __restrict__ windows) {
-  __shared__ xyzz<F> sm[128];
-  const int w = blockIdx.x, t = threadIdx.x;
-  xyzz<F> acc = xyzz_inf<F>();
-  for (size_t j = t; j < J; j += blockDim.x) acc = xyzz_add(acc, ld_pod(contrib + (size_t)w * J + j));
-  sm[t] = acc;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (t < s) sm[t] = xyzz_add(sm[t], sm[t + s]);
-    __syncthreads();
+__global__ void __launch_bounds__(128) k_msm_reduce_up(const xyzz<F>* __restrict__ run_in,
+                                                       const xyzz<F>* __restrict__ acc_in,
+                                                       uint32_t Jin, uint32_t G, int log_span,
+                                                       uint32_t Jout, int W,
+                                                       xyzz<F>* __restrict__ run_out,
+                                                       xyzz<F>* __restrict__ acc_out) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)W * Jout) return;
+  const int w = (int)(t / Jout);
+  const uint32_t first = (uint32_t)(t % Jout) * G;
+  const uint32_t last = min(first + G, Jin) - 1;
+  const size_t base = (size_t)w * Jin;
+  // two live sums at a time (keeps the G2 variant within registers)
+  xyzz<F> r = xyzz_inf<F>(), s = xyzz_inf<F>();
+  for (uint32_t i = last; i > first; i--) {
+    r = xyzz_add(r, ld_pod(run_in + base + i));
+    s = xyzz_add(s, r);  // s = sum_i (i - first) run_i
   }
-  if (t == 0) st_pod(&windows[w], sm[0]);
+  r = xyzz_add(r, ld_pod(run_in + base + first));
+  st_pod(&run_out[t], r);
+  for (int d = 0; d < log_span; d++) s = xyzz_dbl(s);
+  for (uint32_t i = first; i <= last; i++) s = xyzz_add(s, ld_pod(acc_in + base + i));
+  st_pod(&acc_out[t], s);
 }
 
-// --------------------------------------------------------------- driver
+// ------------------------------------------------------ fixed-base tables
+// table record (w * n + i) = affine 2^(c w) P_i, stored (x, y) like a zkey
+// section, for w < W = 254 / c + 1.  With these, all windows of a fixed-base
+// MSM share one bucket set: one bucket reduction instead of W, and no
+// doubling chain between windows.
+template <class F>
+__global__ void __launch_bounds__(128) k_msm_precompute(const F* __restrict__ px,
+                                                        const F* __restrict__ py, uint32_t pstride,
+                                                        size_t n, int c, int W,
+                                                        F* __restrict__ table) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const F x = ld_pod(px + i * pstride), y = ld_pod(py + i * pstride);
+  st_pod(table + 2 * i, x);
+  st_pod(table + 2 * i + 1, y);
+  xyzz<F> acc;
+  const bool inf = fe_is_zero(x) && fe_is_zero(y);
+  if (!inf) acc = xyzz<F>{x, y, fe_one_of<F>(), fe_one_of<F>()};
+  for (int w = 1; w < W; w++) {
+    affine<F> a{fe_zero_of<F>(), fe_zero_of<F>()};
+    if (!inf) {
+      for (int d = 0; d < c; d++) acc = xyzz_dbl(acc);
+      a = xyzz_to_affine(acc);
+    }
+    const size_t rec = (size_t)w * n + i;
+    st_pod(table + 2 * rec, a.x);
+    st_pod(table + 2 * rec + 1, a.y);
+  }
+}
+
+
 template <class F>
 int msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
                 size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t st, const void** d_windows,
-                int* c_out) {
+                int* c_out, bool fixed = false) {
   constexpr bool g2 = sizeof(F) == 64;
   ZK_REQUIRE(n < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
-  const Shape s = make_shape(n, g2, cfg);
+  const Shape s = make_shape(n, g2, cfg, fixed);
+  ZK_REQUIRE(!fixed || (size_t)s.W * n < (size_t(1) << 31), ZK_EINVAL,
+             "msm: fixed-base table too large (windows x points >= 2^31)");
   ZK_REQUIRE(s.c >= 4 && s.c <= 24, ZK_EINVAL, "msm: window size must be in [4, 24]");
   ZK_REQUIRE(s.records < (size_t(1) << 32) - 1, ZK_EINVAL, "msm: too many (point, window) records");
   Layout<F> L = carve<F>(scratch, s);
   ZK_REQUIRE(L.bytes <= scratch_bytes, ZK_EINVAL, "msm: scratch buffer too small");
 
   ZK_CUDA(cudaMemsetAsync(L.counts, 0, s.entries * sizeof(uint32_t), st));
-  ZK_CUDA(cudaMemsetAsync(L.buckets, 0, (size_t)s.W * s.B * sizeof(xyzz<F>), st));
+  ZK_CUDA(cudaMemsetAsync(L.buckets, 0, (size_t)s.Wk * s.B * sizeof(xyzz<F>), st));
   if (n) {
     const int th = 256;
     const unsigned g = (unsigned)((n + th - 1) / th);
-    k_msm_hist<<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
+    if (fixed)
+      k_msm_hist<true><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
+    else
+      k_msm_hist<false><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
     ZK_LAUNCHED();
   }
   scan::exclusive(L.counts, L.cursor, s.entries, L.tiles, st);
   if (n) {
     const int th = 256;
     const unsigned g = (unsigned)((n + th - 1) / th);
-    k_msm_scatter<<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
+    if (fixed)
+      k_msm_scatter<true><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
+    else
+      k_msm_scatter<false><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
     ZK_LAUNCHED();
   }
   const uint32_t* total_p = L.counts + (s.entries - 1);
@@ -484,16 +568,31 @@ int msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* 
     ZK_LAUNCHED();
   }
   {
-    const size_t tot = (size_t)s.W * s.J;
-    k_msm_bucket_reduce<F><<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(L.buckets, s.c, s.W, s.B,
-                                                                           s.chunk, s.J, L.contrib);
+    uint32_t J = s.J;
+    const uint32_t Lc = (uint32_t)s.chunk, G = (uint32_t)s.chunk;
+    int log_span = 0;
+    while ((1u << log_span) < Lc) log_span++;
+    const int log_g = log_span;
+    size_t tot = (size_t)s.Wk * J;
+    k_msm_reduce_l1<F><<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(
+        L.buckets, s.fixed ? 0 : s.c, s.Wk, s.B, Lc, J, L.rrun[0], L.racc[0]);
     ZK_LAUNCHED();
-    k_msm_window_reduce<F><<<s.W, 128, 0, st>>>(L.contrib, s.J, L.windows);
-    ZK_LAUNCHED();
+    int cur = 0;
+    while (J > 1) {
+      const uint32_t Jout = (J + G - 1) / G;
+      tot = (size_t)s.Wk * Jout;
+      k_msm_reduce_up<F><<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(
+          L.rrun[cur], L.racc[cur], J, G, log_span, Jout, s.Wk, L.rrun[cur ^ 1], L.racc[cur ^ 1]);
+      ZK_LAUNCHED();
+      cur ^= 1;
+      J = Jout;
+      log_span += log_g;
+    }
+    L.windows = L.racc[cur];
   }
   *d_windows = L.windows;
   *c_out = s.c;
-  return s.W;
+  return s.Wk;
 }
 
 }  // namespace
@@ -512,6 +611,44 @@ size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg) {
   const Shape s = make_shape(n, g2, cfg);
   if (g2) return carve<fp2_t>(nullptr, s).bytes;
   return carve<fp_t>(nullptr, s).bytes;
+}
+
+size_t msm_table_bytes(size_t n, bool g2, int c) {
+  return (size_t)(254 / c + 1) * n * (g2 ? 128 : 64);
+}
+
+size_t msm_scratch_bytes_fixed(size_t n, bool g2, int c, const MsmConfig& cfg) {
+  MsmConfig k = cfg;
+  k.c = c;
+  const Shape s = make_shape(n, g2, k, true);
+  if (g2) return carve<fp2_t>(nullptr, s).bytes;
+  return carve<fp_t>(nullptr, s).bytes;
+}
+
+void msm_precompute(bool g2, const PointsView& pts, size_t n, int c, void* table, cudaStream_t st) {
+  ZK_REQUIRE(c >= 4 && c <= 24, ZK_EINVAL, "msm table: window size must be in [4, 24]");
+  if (!n) return;
+  const int W = 254 / c + 1;
+  const unsigned g = (unsigned)((n + 127) / 128);
+  if (g2)
+    k_msm_precompute<fp2_t><<<g, 128, 0, st>>>(reinterpret_cast<const fp2_t*>(pts.x),
+                                               reinterpret_cast<const fp2_t*>(pts.y), pts.stride, n,
+                                               c, W, reinterpret_cast<fp2_t*>(table));
+  else
+    k_msm_precompute<fp_t><<<g, 128, 0, st>>>(reinterpret_cast<const fp_t*>(pts.x),
+                                              reinterpret_cast<const fp_t*>(pts.y), pts.stride, n,
+                                              c, W, reinterpret_cast<fp_t*>(table));
+  ZK_LAUNCHED();
+}
+
+int msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
+                      void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st,
+                      const void** d_windows, int* c_out) {
+  MsmConfig k = cfg;
+  k.c = c;
+  const PointsView pts = points_aos(table, g2);
+  if (g2) return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, k, st, d_windows, c_out, true);
+  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, k, st, d_windows, c_out, true);
 }
 
 int msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,

@@ -64,6 +64,20 @@ int msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, voi
                    size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
                    const void** d_windows, int* c_out);
 
+// Fixed-base MSMs: precomputed window multiples of a resident base set.
+// msm_precompute writes W = 254 / c + 1 records per point (table layout:
+// record w * n + i = affine 2^(c w) P_i, (x, y) interleaved); the fixed-base
+// enqueue then sorts all (point, window) digits into one shared bucket set and
+// returns a single window sum (combine it with n_windows = 1).  Scalars are
+// reduced mod r first, which requires points of order r (CRS points are).
+size_t msm_table_bytes(size_t n, bool g2, int c);
+size_t msm_scratch_bytes_fixed(size_t n, bool g2, int c, const MsmConfig& cfg);
+void msm_precompute(bool g2, const PointsView& pts, size_t n, int c, void* table,
+                    cudaStream_t stream);
+int msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
+                      void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
+                      cudaStream_t stream, const void** d_windows, int* c_out);
+
 // Host combination of W window sums (XYZZ, as copied from the device) into an
 // affine Montgomery point.  Returns true for the point at infinity.
 bool msm_g1_combine(const void* h_windows, int n_windows, int c, uint64_t out[8]);

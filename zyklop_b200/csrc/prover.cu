@@ -213,6 +213,38 @@ zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
   return c.release();
 }
 
+int msm_fixed_default_c(size_t n, bool g2) {
+  int lg = 0;
+  while ((size_t(1) << lg) < n) lg++;
+  int c = lg;
+  (void)g2;
+  if (c < 8) c = 8;
+  if (c > 20) c = 20;
+  return c;
+}
+
+void circuit_precompute(zk_circuit* c, int c_g1, int c_g2) {
+  zk_ctx* ctx = c->ctx;
+  cudaStream_t st = ctx->stream;
+  const size_t m1 = c->m1, nc = (size_t)c->m1 - c->l - 1, n = c->n;
+  const int g1c = c_g1 ? c_g1 : msm_fixed_default_c(m1 + 1, false);
+  const int g2c = c_g2 ? c_g2 : msm_fixed_default_c(m1 + 1, true);
+  ZK_REQUIRE(g1c >= 4 && g1c <= 22 && g2c >= 4 && g2c <= 22, ZK_EINVAL,
+             "precompute: window bits must be in [4, 22]");
+  auto build = [&](DeviceBuffer& tab, const DeviceBuffer& pts, size_t cnt, bool g2, int cb) {
+    tab.ensure(msm_table_bytes(cnt ? cnt : 1, g2, cb));
+    msm_precompute(g2, points_aos(pts.ptr, g2), cnt, cb, tab.ptr, st);
+  };
+  build(c->tab_a, c->pts_a, m1 + 1, false, g1c);
+  build(c->tab_b2, c->pts_b2, m1 + 1, true, g2c);
+  build(c->tab_c_pts, c->pts_c, nc, false, g1c);
+  build(c->tab_h, c->pts_h, n, false, g1c);
+  if (c->has_b1) build(c->tab_b1, c->pts_b1, m1 + 1, false, g1c);
+  ZK_CUDA(cudaStreamSynchronize(st));
+  c->tab_c[0] = g1c;
+  c->tab_c[1] = g2c;
+}
+
 void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_device,
            const uint64_t* r, const uint64_t* s, uint64_t proof[32], ProveIntermediates* dbg) {
   zk_ctx* ctx = c->ctx;
@@ -231,10 +263,14 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   ctx->ntt.ensure(c->log_n, ws.st[0]);
   const MsmConfig& c1 = ctx->msm_cfg[0];
   const MsmConfig& c2 = ctx->msm_cfg[1];
-  const size_t need[ProveWs::kStreams] = {
-      msm_scratch_bytes(n, false, c1), msm_scratch_bytes(m1 + 1, false, c1),
-      msm_scratch_bytes(m1 + 1, true, c2), msm_scratch_bytes(nc, false, c1),
-      blind ? msm_scratch_bytes(m1 + 1, false, c1) : 0};
+  const bool fixed = c->tab_c[0] != 0;
+  auto scratch = [&](size_t cnt, bool g2) {
+    return fixed ? msm_scratch_bytes_fixed(cnt, g2, c->tab_c[g2 ? 1 : 0], g2 ? c2 : c1)
+                 : msm_scratch_bytes(cnt, g2, g2 ? c2 : c1);
+  };
+  const size_t need[ProveWs::kStreams] = {scratch(n, false), scratch(m1 + 1, false),
+                                          scratch(m1 + 1, true), scratch(nc, false),
+                                          blind ? scratch(m1 + 1, false) : 0};
   for (int i = 0; i < ProveWs::kStreams; i++)
     if (need[i]) {
       if (ws.msm[i].cap < need[i]) ZK_CUDA(cudaStreamSynchronize(ws.st[i]));
@@ -260,20 +296,28 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   // 2. MSMs that only need the witness, on their own streams
   const void* dwin[ProveWs::kStreams] = {};
   int W[ProveWs::kStreams] = {}, C[ProveWs::kStreams] = {};
-  auto launch = [&](int i, bool g2, const PointsView& pts, const uint64_t* sc, size_t cnt) {
+  auto launch = [&](int i, bool g2, const DeviceBuffer& pts, const DeviceBuffer& tab,
+                    const uint64_t* sc, size_t cnt) {
     cudaStream_t st = ws.st[i];
     if (i) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
-    W[i] = g2 ? msm_g2_enqueue(pts, sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c2, st, &dwin[i], &C[i])
-              : msm_g1_enqueue(pts, sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c1, st, &dwin[i], &C[i]);
+    if (fixed)
+      W[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
+                               ws.msm[i].cap, g2 ? c2 : c1, st, &dwin[i], &C[i]);
+    else if (g2)
+      W[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c2, st,
+                            &dwin[i], &C[i]);
+    else
+      W[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c1,
+                            st, &dwin[i], &C[i]);
     const size_t bytes = (size_t)W[i] * (g2 ? 256 : 128);
     ws.win[i].ensure(bytes);
     ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, dwin[i], bytes, cudaMemcpyDeviceToHost, st));
     ZK_CUDA(cudaEventRecord(ws.ev_done[i], st));
   };
-  launch(1, false, points_aos(c->pts_a.ptr, false), we, m1 + 1);
-  launch(2, true, points_aos(c->pts_b2.ptr, true), we, m1 + 1);
-  launch(3, false, points_aos(c->pts_c.ptr, false), we + 4 * (l + 2), nc);
-  if (blind) launch(4, false, points_aos(c->pts_b1.ptr, false), we, m1 + 1);
+  launch(1, false, c->pts_a, c->tab_a, we, m1 + 1);
+  launch(2, true, c->pts_b2, c->tab_b2, we, m1 + 1);
+  launch(3, false, c->pts_c, c->tab_c_pts, we + 4 * (l + 2), nc);
+  if (blind) launch(4, false, c->pts_b1, c->tab_b1, we, m1 + 1);
 
   // 3. SpMV -> H -> MSM_H on stream 0
   SpmvArgs sa;
@@ -302,7 +346,7 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
     ZK_CUDA(cudaMemcpyAsync(dbg->h, ws.h.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
     ZK_CUDA(cudaStreamSynchronize(s0));
   }
-  launch(0, false, points_aos(c->pts_h.ptr, false), ws.h.as<uint64_t>(), n);
+  launch(0, false, c->pts_h, c->tab_h, ws.h.as<uint64_t>(), n);
 
   // 4. host: combine the window sums, assemble the proof
   const int used = blind ? 5 : 4;

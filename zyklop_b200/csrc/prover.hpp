@@ -35,6 +35,17 @@ struct zk_circuit {
   zk::DeviceBuffer pts_a, pts_b1, pts_b2, pts_c, pts_h;
   // CSR of the A and B matrices: row pointers (n + 1), signal ids, coef * R^2
   zk::DeviceBuffer row[2], sig[2], val[2];
+  // optional fixed-base tables (window multiples) of the point sets above,
+  // window bits per group (0: not built)
+  int tab_c[2] = {0, 0};
+  zk::DeviceBuffer tab_a, tab_b1, tab_b2, tab_c_pts, tab_h;
+};
+
+struct zk_msm_table {
+  zk_ctx* ctx = nullptr;
+  int group = 1, c = 0;
+  size_t n = 0;
+  zk::DeviceBuffer table;
 };
 
 namespace zk {
@@ -48,6 +59,13 @@ struct ProveIntermediates {
   uint64_t* bw = nullptr;  // host, domain x 4 (Montgomery B.w)
   uint64_t* h = nullptr;   // host, domain x 4 (canonical h)
 };
+
+// Builds fixed-base tables for every point set of the circuit (c_g1 / c_g2
+// window bits; 0 picks the default for the set's size).
+void circuit_precompute(zk_circuit* c, int c_g1, int c_g2);
+
+// Default window bits of a fixed-base MSM over n points.
+int msm_fixed_default_c(size_t n, bool g2);
 
 // Proves with a witness of >= m1 canonical Fr values (host or device memory).
 // r / s: canonical Fr blinding scalars or nullptr (reference behaviour).
