@@ -59,6 +59,7 @@ def parse_args():
     p.add_argument("--witness", choices=["uniform", "circom"], default="uniform")
     p.add_argument("--e2e-steps", type=int, default=0, help="default: min(steps, 5)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--table-c", default="0,0", help="fixed-base window bits G1,G2 (0 = default)")
     p.add_argument("--workdir", default=os.environ.get("ZK_BENCH_DIR", "/tmp/zyklop_bench"))
     return p.parse_args()
 
@@ -229,7 +230,8 @@ def run_mine(args, dist):
     check(L.zk_ctx_set_stream(ctx, ctypes.c_void_p(stream.cuda_stream)))
     circuit = api.Circuit(z, ctx=ctx)
     t_pre = time.perf_counter()
-    circuit.precompute()  # fixed-base window tables for the resident CRS
+    tc = [int(x) for x in args.table_c.split(",")]
+    circuit.precompute(tc[0], tc[1])  # fixed-base window tables for the resident CRS
     t_pre = time.perf_counter() - t_pre
     wit = api.read_wtns(w)
     dwit = api.to_device(wit)

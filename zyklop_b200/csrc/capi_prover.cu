@@ -110,14 +110,13 @@ int zk_msm_table_run(zk_msm_table* t, const uint64_t* d_scalars, size_t n, uint6
     scal = sc.as<uint64_t>();
   }
   ctx->msm_scratch.ensure(msm_scratch_bytes_fixed(cnt, g2, t->c, cfg));
-  const void* dw;
-  int cc;
-  const int W = msm_enqueue_fixed(g2, t->table.ptr, scal, cnt, t->c, ctx->msm_scratch.ptr,
-                                  ctx->msm_scratch.cap, cfg, ctx->stream, &dw, &cc);
-  uint8_t h[512];
-  ZK_CUDA(cudaMemcpyAsync(h, dw, (size_t)W * (g2 ? 256 : 128), cudaMemcpyDeviceToHost, ctx->stream));
+  const MsmResult r = msm_enqueue_fixed(g2, t->table.ptr, scal, cnt, t->c, ctx->msm_scratch.ptr,
+                                        ctx->msm_scratch.cap, cfg, ctx->stream);
+  alignas(16) uint8_t h[1024];
+  ZK_REQUIRE(r.bytes <= sizeof(h), ZK_EINTERNAL, "zk_msm_table_run: result too large");
+  ZK_CUDA(cudaMemcpyAsync(h, r.d_data, r.bytes, cudaMemcpyDeviceToHost, ctx->stream));
   ZK_CUDA(cudaStreamSynchronize(ctx->stream));
-  const bool inf = g2 ? msm_g2_combine(h, W, cc, h_out) : msm_g1_combine(h, W, cc, h_out);
+  const bool inf = g2 ? msm_g2_combine(h, r, h_out) : msm_g1_combine(h, r, h_out);
   if (is_inf) *is_inf = inf ? 1 : 0;
   ZK_API_END
 }

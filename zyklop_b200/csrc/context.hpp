@@ -15,6 +15,7 @@ namespace zk {
 struct ProveWs {
   static constexpr int kStreams = 5;  // 0: witness/SpMV/H/MSM_H, 1: A, 2: B2, 3: C, 4: B1
   bool ready = false;
+  int nstreams = kStreams;
   cudaStream_t st[kStreams] = {};
   cudaEvent_t ev_we = nullptr, ev_begin = nullptr;
   cudaEvent_t ev_done[kStreams] = {};

@@ -18,6 +18,7 @@ namespace {
 
 constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr uint32_t kNeg = 0x80000000u;
+constexpr int kRedT = 128;  // pairs per block in the bucket-reduction block passes
 
 // ------------------------------------------------------------------ shape
 struct Shape {
@@ -80,7 +81,7 @@ struct Layout {
   xyzz<F>* ppt[2];
   xyzz<F>* rrun[2];   // bucket-reduction (run, acc) pairs, ping-pong
   xyzz<F>* racc[2];
-  xyzz<F>* windows;   // W window sums (points into racc)
+  xyzz<F>* outua;     // 2 * W: U_0..U_{W-1}, A_0..A_{W-1}
   size_t bytes;
 };
 
@@ -100,12 +101,12 @@ Layout<F> carve(void* base, const Shape& s) {
     L.pkey[i] = cv.take<uint32_t>(pmax[i]);
     L.ppt[i] = cv.take<xyzz<F>>(pmax[i]);
   }
-  const size_t j2 = (s.J + s.chunk - 1) / s.chunk;
+  const size_t j2 = (s.J + kRedT - 1) / kRedT;
   L.rrun[0] = cv.take<xyzz<F>>((size_t)s.Wk * s.J);
   L.racc[0] = cv.take<xyzz<F>>((size_t)s.Wk * s.J);
   L.rrun[1] = cv.take<xyzz<F>>((size_t)s.Wk * j2);
   L.racc[1] = cv.take<xyzz<F>>((size_t)s.Wk * j2);
-  L.windows = nullptr;
+  L.outua = cv.take<xyzz<F>>((size_t)s.Wk * 2);
   L.bytes = cv.off + 256;
   return L;
 }
@@ -424,14 +425,19 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accumN(
 }
 
 // ------------------------------------------------------ bucket reduction
-// Window sums sum_b (b+1) S_b without per-chunk scalar multiplications.
+// Window sums sum_b (b+1) S_b, without per-chunk scalar multiplications and
+// without long serial chains above the first level.
+//
 // Level 1: thread per (window, chunk of L buckets) -> (run, acc) with
 // run = sum S_b and acc = sum (i+1) S_{lo+i} (running sums from the top).
-// Level k > 1: thread per (window, group of G consecutive level-(k-1) pairs,
-// each covering `span` buckets) -> run' = sum run_i and
-// acc' = sum acc_i + span * sum_i i run_i, where sum_i i run_i is again a
-// running sum and span is a power of two (log2(span) doublings).  The last
-// level leaves one pair per window; its acc is the window sum.
+// Block passes: block per (window, segment of up to kRedT consecutive pairs,
+// each covering 2^log_span buckets) -> run' = sum run_i and
+// acc' = sum acc_i + 2^log_span * sum_i i run_i.  In the block,
+// sum_i i run_i = sum_{i>=1} S_i with S_i = sum_{k>=i} run_k: a shared-memory
+// suffix scan (log2 kRedT steps) and a tree reduction, so the depth is
+// logarithmic.  The final pass (one segment per window) stops before the
+// doublings and leaves U = sum_i i run_i and A = sum_i acc_i; the host forms
+// the window sum A + 2^log_span U, where a serial doubling chain is cheap.
 template <class F>
 __global__ void __launch_bounds__(128) k_msm_reduce_l1(const xyzz<F>* __restrict__ buckets, int c,
                                                        int W, uint32_t B, uint32_t L, uint32_t J,
@@ -457,30 +463,57 @@ __global__ void __launch_bounds__(128) k_msm_reduce_l1(const xyzz<F>* __restrict
   st_pod(&acc_out[t], acc);
 }
 
+// block tree sum of one value per thread (result valid in thread 0)
 template <class F>
-__global__ void __launch_bounds__(128) k_msm_reduce_up(const xyzz<F>* __restrict__ run_in,
-                                                       const xyzz<F>* __restrict__ acc_in,
-                                                       uint32_t Jin, uint32_t G, int log_span,
-                                                       uint32_t Jout, int W,
-                                                       xyzz<F>* __restrict__ run_out,
-                                                       xyzz<F>* __restrict__ acc_out) {
-  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (size_t)W * Jout) return;
-  const int w = (int)(t / Jout);
-  const uint32_t first = (uint32_t)(t % Jout) * G;
-  const uint32_t last = min(first + G, Jin) - 1;
-  const size_t base = (size_t)w * Jin;
-  // two live sums at a time (keeps the G2 variant within registers)
-  xyzz<F> r = xyzz_inf<F>(), s = xyzz_inf<F>();
-  for (uint32_t i = last; i > first; i--) {
-    r = xyzz_add(r, ld_pod(run_in + base + i));
-    s = xyzz_add(s, r);  // s = sum_i (i - first) run_i
+__device__ __forceinline__ xyzz<F> block_sum(xyzz<F> v, xyzz<F>* sm) {
+  const int i = threadIdx.x;
+  sm[i] = v;
+  __syncthreads();
+  for (int s = kRedT / 2; s > 0; s >>= 1) {
+    if (i < s) sm[i] = xyzz_add(sm[i], sm[i + s]);
+    __syncthreads();
   }
-  r = xyzz_add(r, ld_pod(run_in + base + first));
-  st_pod(&run_out[t], r);
-  for (int d = 0; d < log_span; d++) s = xyzz_dbl(s);
-  for (uint32_t i = first; i <= last; i++) s = xyzz_add(s, ld_pod(acc_in + base + i));
-  st_pod(&acc_out[t], s);
+  const xyzz<F> r = sm[0];
+  __syncthreads();
+  return r;
+}
+
+// grid (segments, windows); out_u / out_a receive U and A of final passes
+template <class F>
+__global__ void __launch_bounds__(kRedT) k_msm_reduce_blk(
+    const xyzz<F>* __restrict__ run_in, const xyzz<F>* __restrict__ acc_in, uint32_t Jin,
+    int log_span, uint32_t Jout, xyzz<F>* __restrict__ run_out, xyzz<F>* __restrict__ acc_out,
+    xyzz<F>* __restrict__ out_u, xyzz<F>* __restrict__ out_a) {
+  __shared__ xyzz<F> sm[kRedT];
+  const int w = blockIdx.y, i = threadIdx.x;
+  const uint32_t idx = blockIdx.x * kRedT + i;
+  const size_t base = (size_t)w * Jin;
+  xyzz<F> r = idx < Jin ? ld_pod(run_in + base + idx) : xyzz_inf<F>();
+  // inclusive suffix scan: r = S_i = sum_{k >= i} run_k within the segment
+  sm[i] = r;
+  __syncthreads();
+  for (int off = 1; off < kRedT; off <<= 1) {
+    const xyzz<F> o = i + off < kRedT ? sm[i + off] : xyzz_inf<F>();
+    __syncthreads();
+    r = xyzz_add(r, o);
+    sm[i] = r;
+    __syncthreads();
+  }
+  const xyzz<F> total = sm[0];  // S_0 = sum of the segment's runs
+  __syncthreads();
+  const xyzz<F> u = block_sum<F>(i >= 1 ? r : xyzz_inf<F>(), sm);
+  const xyzz<F> a = block_sum<F>(idx < Jin ? ld_pod(acc_in + base + idx) : xyzz_inf<F>(), sm);
+  if (i != 0) return;
+  if (Jout == 1) {
+    st_pod(&out_u[w], u);
+    st_pod(&out_a[w], a);
+    return;
+  }
+  xyzz<F> x = u;
+  for (int d = 0; d < log_span; d++) x = xyzz_dbl(x);
+  const size_t o = (size_t)w * Jout + blockIdx.x;
+  st_pod(&run_out[o], total);
+  st_pod(&acc_out[o], xyzz_add(a, x));
 }
 
 // ------------------------------------------------------ fixed-base tables
@@ -515,9 +548,9 @@ __global__ void __launch_bounds__(128) k_msm_precompute(const F* __restrict__ px
 
 
 template <class F>
-int msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t st, const void** d_windows,
-                int* c_out, bool fixed = false) {
+MsmResult msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                      size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t st,
+                      bool fixed = false) {
   constexpr bool g2 = sizeof(F) == 64;
   ZK_REQUIRE(n < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
   const Shape s = make_shape(n, g2, cfg, fixed);
@@ -567,32 +600,35 @@ int msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* 
         L.pkey[in], L.ppt[in], s.lvl_records[l], s.k1, L.buckets, ok, L.ppt[out]);
     ZK_LAUNCHED();
   }
+  int log_span = 0;
   {
-    uint32_t J = s.J;
-    const uint32_t Lc = (uint32_t)s.chunk, G = (uint32_t)s.chunk;
-    int log_span = 0;
+    uint32_t J = (uint32_t)s.J;
+    const uint32_t Lc = (uint32_t)s.chunk;
     while ((1u << log_span) < Lc) log_span++;
-    const int log_g = log_span;
-    size_t tot = (size_t)s.Wk * J;
+    const size_t tot = (size_t)s.Wk * J;
     k_msm_reduce_l1<F><<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(
         L.buckets, s.fixed ? 0 : s.c, s.Wk, s.B, Lc, J, L.rrun[0], L.racc[0]);
     ZK_LAUNCHED();
     int cur = 0;
-    while (J > 1) {
-      const uint32_t Jout = (J + G - 1) / G;
-      tot = (size_t)s.Wk * Jout;
-      k_msm_reduce_up<F><<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(
-          L.rrun[cur], L.racc[cur], J, G, log_span, Jout, s.Wk, L.rrun[cur ^ 1], L.racc[cur ^ 1]);
+    for (;;) {
+      const uint32_t Jout = (J + kRedT - 1) / kRedT;
+      k_msm_reduce_blk<F><<<dim3(Jout, s.Wk), kRedT, 0, st>>>(
+          L.rrun[cur], L.racc[cur], J, log_span, Jout, L.rrun[cur ^ 1], L.racc[cur ^ 1], L.outua,
+          L.outua + s.Wk);
       ZK_LAUNCHED();
+      if (Jout == 1) break;
       cur ^= 1;
       J = Jout;
-      log_span += log_g;
+      log_span += 7;  // kRedT = 2^7 pairs per block
     }
-    L.windows = L.racc[cur];
   }
-  *d_windows = L.windows;
-  *c_out = s.c;
-  return s.Wk;
+  MsmResult res;
+  res.d_data = L.outua;
+  res.bytes = (size_t)2 * s.Wk * sizeof(xyzz<F>);
+  res.windows = s.Wk;
+  res.c = s.c;
+  res.log_span = log_span;
+  return res;
 }
 
 }  // namespace
@@ -641,25 +677,22 @@ void msm_precompute(bool g2, const PointsView& pts, size_t n, int c, void* table
   ZK_LAUNCHED();
 }
 
-int msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
-                      void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st,
-                      const void** d_windows, int* c_out) {
+MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
+                            void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
   MsmConfig k = cfg;
   k.c = c;
   const PointsView pts = points_aos(table, g2);
-  if (g2) return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, k, st, d_windows, c_out, true);
-  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, k, st, d_windows, c_out, true);
+  if (g2) return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, k, st, true);
+  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, k, st, true);
 }
 
-int msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                   size_t bytes, const MsmConfig& cfg, cudaStream_t st, const void** d_windows,
-                   int* c_out) {
-  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
+MsmResult msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                         size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
+  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, cfg, st);
 }
-int msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                   size_t bytes, const MsmConfig& cfg, cudaStream_t st, const void** d_windows,
-                   int* c_out) {
-  return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, cfg, st, d_windows, c_out);
+MsmResult msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                         size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
+  return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, cfg, st);
 }
 
 namespace {
@@ -668,18 +701,32 @@ host::Fp fp_from_words(const uint32_t* w) {
   memcpy(r.v, w, 32);
   return r;
 }
+host::Fp2 fp2_from_words(const uint32_t* q) { return host::Fp2{fp_from_words(q), fp_from_words(q + 8)}; }
+
+// window w = A_w + 2^log_span U_w, then Horner over windows with c doublings
+template <class T, class Load>
+host::Xyzz<T> combine(const uint8_t* data, const MsmResult& r, size_t pt_bytes, Load load) {
+  using P = host::Xyzz<T>;
+  P acc = P::inf();
+  for (int w = r.windows - 1; w >= 0; w--) {
+    for (int i = 0; i < r.c && !acc.is_inf(); i++) acc = acc.dbl();
+    P u = load(data + (size_t)w * pt_bytes);
+    const P a = load(data + (size_t)(r.windows + w) * pt_bytes);
+    for (int i = 0; i < r.log_span && !u.is_inf(); i++) u = u.dbl();
+    acc = acc.add(u).add(a);
+  }
+  return acc;
+}
 }  // namespace
 
-bool msm_g1_combine(const void* h_windows, int W, int c, uint64_t out[8]) {
+bool msm_g1_combine(const void* h_data, const MsmResult& r, uint64_t out[8]) {
   using P = host::Xyzz<host::Fp>;
-  const uint32_t* raw = reinterpret_cast<const uint32_t*>(h_windows);
-  P acc = P::inf();
-  for (int w = W - 1; w >= 0; w--) {
-    for (int i = 0; i < c; i++) acc = acc.dbl();
-    const uint32_t* q = raw + (size_t)w * 32;
-    P win{fp_from_words(q), fp_from_words(q + 8), fp_from_words(q + 16), fp_from_words(q + 24)};
-    acc = acc.add(win);
-  }
+  const P acc = combine<host::Fp>(reinterpret_cast<const uint8_t*>(h_data), r, 128,
+                                  [](const uint8_t* p) {
+                                    const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
+                                    return P{fp_from_words(q), fp_from_words(q + 8),
+                                             fp_from_words(q + 16), fp_from_words(q + 24)};
+                                  });
   host::Fp x, y;
   const bool inf = acc.to_affine(x, y);
   memcpy(out, x.v, 32);
@@ -687,17 +734,14 @@ bool msm_g1_combine(const void* h_windows, int W, int c, uint64_t out[8]) {
   return inf;
 }
 
-bool msm_g2_combine(const void* h_windows, int W, int c, uint64_t out[16]) {
+bool msm_g2_combine(const void* h_data, const MsmResult& r, uint64_t out[16]) {
   using P = host::Xyzz<host::Fp2>;
-  const uint32_t* raw = reinterpret_cast<const uint32_t*>(h_windows);
-  auto f2 = [](const uint32_t* q) { return host::Fp2{fp_from_words(q), fp_from_words(q + 8)}; };
-  P acc = P::inf();
-  for (int w = W - 1; w >= 0; w--) {
-    for (int i = 0; i < c; i++) acc = acc.dbl();
-    const uint32_t* q = raw + (size_t)w * 64;
-    P win{f2(q), f2(q + 16), f2(q + 32), f2(q + 48)};
-    acc = acc.add(win);
-  }
+  const P acc = combine<host::Fp2>(reinterpret_cast<const uint8_t*>(h_data), r, 256,
+                                   [](const uint8_t* p) {
+                                     const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
+                                     return P{fp2_from_words(q), fp2_from_words(q + 16),
+                                              fp2_from_words(q + 32), fp2_from_words(q + 48)};
+                                   });
   host::Fp2 x, y;
   const bool inf = acc.to_affine(x, y);
   memcpy(out, x.c0.v, 32);
@@ -710,25 +754,21 @@ bool msm_g2_combine(const void* h_windows, int W, int c, uint64_t out[16]) {
 bool msm_g1_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,
                 const MsmConfig& cfg, cudaStream_t st, uint64_t out[8]) {
   scratch.ensure(msm_scratch_bytes(n, false, cfg));
-  const void* dw;
-  int c;
-  const int W = msm_g1_enqueue(pts, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
-  std::vector<uint8_t> h((size_t)W * 128);
-  ZK_CUDA(cudaMemcpyAsync(h.data(), dw, h.size(), cudaMemcpyDeviceToHost, st));
+  const MsmResult r = msm_g1_enqueue(pts, scalars, n, scratch.ptr, scratch.cap, cfg, st);
+  std::vector<uint8_t> h(r.bytes);
+  ZK_CUDA(cudaMemcpyAsync(h.data(), r.d_data, r.bytes, cudaMemcpyDeviceToHost, st));
   ZK_CUDA(cudaStreamSynchronize(st));
-  return msm_g1_combine(h.data(), W, c, out);
+  return msm_g1_combine(h.data(), r, out);
 }
 
 bool msm_g2_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,
                 const MsmConfig& cfg, cudaStream_t st, uint64_t out[16]) {
   scratch.ensure(msm_scratch_bytes(n, true, cfg));
-  const void* dw;
-  int c;
-  const int W = msm_g2_enqueue(pts, scalars, n, scratch.ptr, scratch.cap, cfg, st, &dw, &c);
-  std::vector<uint8_t> h((size_t)W * 256);
-  ZK_CUDA(cudaMemcpyAsync(h.data(), dw, h.size(), cudaMemcpyDeviceToHost, st));
+  const MsmResult r = msm_g2_enqueue(pts, scalars, n, scratch.ptr, scratch.cap, cfg, st);
+  std::vector<uint8_t> h(r.bytes);
+  ZK_CUDA(cudaMemcpyAsync(h.data(), r.d_data, r.bytes, cudaMemcpyDeviceToHost, st));
   ZK_CUDA(cudaStreamSynchronize(st));
-  return msm_g2_combine(h.data(), W, c, out);
+  return msm_g2_combine(h.data(), r, out);
 }
 
 }  // namespace zk

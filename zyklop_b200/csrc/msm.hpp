@@ -31,7 +31,7 @@ namespace zk {
 
 struct MsmConfig {
   int c = 0;          // window bits (0 = choose from n)
-  int k0 = 32;        // sorted records per thread in the first accumulation level
+  int k0 = 64;        // sorted records per thread in the first accumulation level
   int k1 = 16;        // partial records per thread in later levels
   int chunk = 16;     // buckets per thread in the bucket reduction
 };
@@ -49,20 +49,28 @@ inline PointsView points_aos(const void* base, bool g2) {
   return {base, reinterpret_cast<const char*>(base) + (g2 ? 64 : 32), 2};
 }
 
+// Where an enqueued MSM leaves its result: per window w two XYZZ points U_w
+// and A_w (all U first, then all A) with window sum A_w + 2^log_span U_w, and
+// the total sum_w 2^(c w) window_w.  windows = 1 for fixed-base MSMs.
+struct MsmResult {
+  const void* d_data = nullptr;
+  size_t bytes = 0;
+  int windows = 0;
+  int c = 0;
+  int log_span = 0;
+};
+
 int msm_default_c(size_t n, bool g2);
 
 // Device scratch bytes one MSM of n points needs with this configuration.
 size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg);
 
-// Enqueue the GPU part of an MSM on `stream`; the W window sums (XYZZ) land
-// in the returned device pointer inside `scratch`.  `scratch` must hold
-// msm_scratch_bytes(n, ...) bytes.  Returns the number of windows.
-int msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                   size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
-                   const void** d_windows, int* c_out);
-int msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                   size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
-                   const void** d_windows, int* c_out);
+// Enqueue the GPU part of an MSM on `stream`; its result stays inside
+// `scratch` (which must hold msm_scratch_bytes(n, ...) bytes) until copied.
+MsmResult msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                         size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream);
+MsmResult msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                         size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream);
 
 // Fixed-base MSMs: precomputed window multiples of a resident base set.
 // msm_precompute writes W = 254 / c + 1 records per point (table layout:
@@ -74,14 +82,14 @@ size_t msm_table_bytes(size_t n, bool g2, int c);
 size_t msm_scratch_bytes_fixed(size_t n, bool g2, int c, const MsmConfig& cfg);
 void msm_precompute(bool g2, const PointsView& pts, size_t n, int c, void* table,
                     cudaStream_t stream);
-int msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
-                      void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
-                      cudaStream_t stream, const void** d_windows, int* c_out);
+MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
+                            void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
+                            cudaStream_t stream);
 
-// Host combination of W window sums (XYZZ, as copied from the device) into an
+// Host combination of an MSM result (r.bytes copied from r.d_data) into an
 // affine Montgomery point.  Returns true for the point at infinity.
-bool msm_g1_combine(const void* h_windows, int n_windows, int c, uint64_t out[8]);
-bool msm_g2_combine(const void* h_windows, int n_windows, int c, uint64_t out[16]);
+bool msm_g1_combine(const void* h_data, const MsmResult& r, uint64_t out[8]);
+bool msm_g2_combine(const void* h_data, const MsmResult& r, uint64_t out[16]);
 
 // Blocking convenience wrappers: enqueue, copy the window sums back, combine.
 bool msm_g1_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,

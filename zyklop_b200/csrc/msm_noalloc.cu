@@ -86,15 +86,13 @@ extern "C" int zk_msm_g1_noalloc(const uint64_t* d_px, const uint64_t* d_py,
   ZK_REQUIRE(zk::msm_scratch_bytes(n, false, cfg) <= kNoAllocScratchBytes, ZK_EINTERNAL,
              "zk_msm_g1_noalloc: scratch layout exceeds the fixed array");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const void* d_windows = nullptr;
-  int c = 0;
-  const int W = zk::msm_g1_enqueue(zk::points_soa(d_px, d_py), d_scalars, n, scratch,
-                                   kNoAllocScratchBytes, cfg, st, &d_windows, &c);
-  ZK_REQUIRE(W <= kMaxWindows, ZK_EINTERNAL, "zk_msm_g1_noalloc: too many windows");
-  alignas(16) unsigned char h_windows[kMaxWindows * 128];
-  ZK_CUDA(cudaMemcpyAsync(h_windows, d_windows, (size_t)W * 128, cudaMemcpyDeviceToHost, st));
+  const zk::MsmResult r = zk::msm_g1_enqueue(zk::points_soa(d_px, d_py), d_scalars, n, scratch,
+                                             kNoAllocScratchBytes, cfg, st);
+  alignas(16) unsigned char h_windows[2 * kMaxWindows * 128];
+  ZK_REQUIRE(r.bytes <= sizeof(h_windows), ZK_EINTERNAL, "zk_msm_g1_noalloc: too many windows");
+  ZK_CUDA(cudaMemcpyAsync(h_windows, r.d_data, r.bytes, cudaMemcpyDeviceToHost, st));
   ZK_CUDA(cudaStreamSynchronize(st));
-  const bool inf = zk::msm_g1_combine(h_windows, W, c, h_out);
+  const bool inf = zk::msm_g1_combine(h_windows, r, h_out);
   if (is_inf) *is_inf = inf ? 1 : 0;
   ZK_API_END
 }

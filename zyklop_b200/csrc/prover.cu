@@ -1,6 +1,7 @@
 // Groth16 prover on sm_100a (see prover.hpp).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -108,6 +109,12 @@ P mul(const P& p, const uint64_t* k) {
 
 void ProveWs::init() {
   if (ready) return;
+  // ZYKLOP_PROVE_STREAMS=1 runs a proof's MSMs back to back on one stream
+  // (a tuning knob: concurrent MSMs share L2 and the SMs)
+  if (const char* e = getenv("ZYKLOP_PROVE_STREAMS")) {
+    const int v = atoi(e);
+    if (v >= 1 && v <= kStreams) nstreams = v;
+  }
   for (int i = 0; i < kStreams; i++) {
     ZK_CUDA(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
     ZK_CUDA(cudaEventCreateWithFlags(&ev_done[i], cudaEventDisableTiming));
@@ -294,24 +301,23 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   ZK_CUDA(cudaEventRecord(ws.ev_we, s0));
 
   // 2. MSMs that only need the witness, on their own streams
-  const void* dwin[ProveWs::kStreams] = {};
-  int W[ProveWs::kStreams] = {}, C[ProveWs::kStreams] = {};
+  MsmResult res[ProveWs::kStreams];
   auto launch = [&](int i, bool g2, const DeviceBuffer& pts, const DeviceBuffer& tab,
                     const uint64_t* sc, size_t cnt) {
-    cudaStream_t st = ws.st[i];
-    if (i) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
+    const int si = i % ws.nstreams;
+    cudaStream_t st = ws.st[si];
+    if (si) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
     if (fixed)
-      W[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
-                               ws.msm[i].cap, g2 ? c2 : c1, st, &dwin[i], &C[i]);
+      res[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
+                                 ws.msm[i].cap, g2 ? c2 : c1, st);
     else if (g2)
-      W[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c2, st,
-                            &dwin[i], &C[i]);
+      res[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c2,
+                              st);
     else
-      W[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c1,
-                            st, &dwin[i], &C[i]);
-    const size_t bytes = (size_t)W[i] * (g2 ? 256 : 128);
-    ws.win[i].ensure(bytes);
-    ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, dwin[i], bytes, cudaMemcpyDeviceToHost, st));
+      res[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap,
+                              c1, st);
+    ws.win[i].ensure(res[i].bytes);
+    ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, res[i].d_data, res[i].bytes, cudaMemcpyDeviceToHost, st));
     ZK_CUDA(cudaEventRecord(ws.ev_done[i], st));
   };
   launch(1, false, c->pts_a, c->tab_a, we, m1 + 1);
@@ -353,14 +359,14 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   for (int i = 0; i < used; i++) ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_done[i], 0));
   for (int i = 0; i < used; i++) ZK_CUDA(cudaEventSynchronize(ws.ev_done[i]));
   uint64_t pa[8], pb[16], pc[8], ph[8], pb1[8];
-  msm_g1_combine(ws.win[1].ptr, W[1], C[1], pa);
-  msm_g2_combine(ws.win[2].ptr, W[2], C[2], pb);
-  msm_g1_combine(ws.win[3].ptr, W[3], C[3], pc);
-  msm_g1_combine(ws.win[0].ptr, W[0], C[0], ph);
+  msm_g1_combine(ws.win[1].ptr, res[1], pa);
+  msm_g2_combine(ws.win[2].ptr, res[2], pb);
+  msm_g1_combine(ws.win[3].ptr, res[3], pc);
+  msm_g1_combine(ws.win[0].ptr, res[0], ph);
   G1 A = g1_aff(pa), Cc = g1_aff(pc).add(g1_aff(ph));
   G2 B = g2_aff(pb);
   if (blind) {
-    msm_g1_combine(ws.win[4].ptr, W[4], C[4], pb1);
+    msm_g1_combine(ws.win[4].ptr, res[4], pb1);
     const G1 d1 = g1_aff(c->delta1);
     A = A.add(mul(d1, r));
     B = B.add(mul(g2_aff(c->delta2), s));
