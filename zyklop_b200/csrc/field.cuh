@@ -230,8 +230,11 @@ __device__ __forceinline__ fe<C> fe_dbl(const fe<C>& a) {
       : "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)      \
       : "n"(C::P1), "n"(C::P3), "n"(C::P5), "n"(C::P7), "r"(M))
 
+// Fully unrolled product (~300 instructions).  Kernels with one or two
+// products per loop body (NTT butterflies, SpMV, elementwise passes) call it
+// directly.
 template <class C>
-__device__ __forceinline__ fe<C> operator*(const fe<C>& a, const fe<C>& b) {
+__device__ __forceinline__ fe<C> fe_mul_inline(const fe<C>& a, const fe<C>& b) {
   uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
@@ -247,6 +250,21 @@ __device__ __forceinline__ fe<C> operator*(const fe<C>& a, const fe<C>& b) {
   fe<C> r{{t0, t1, t2, t3, t4, t5, t6, t7}};
   fe_reduce_once<C>(r.v);
   return r;
+}
+
+// Out-of-line product (arguments and result travel in registers).  Curve
+// formulas use it through operator*: inlining every product of a mixed add,
+// doubling and full add made the MSM kernels several times larger than the
+// instruction cache (ncu: warps stalled on instruction fetch); one shared
+// body per kernel keeps the hot loop resident.
+template <class C>
+__device__ __noinline__ fe<C> fe_mul_call(fe<C> a, fe<C> b) {
+  return fe_mul_inline(a, b);
+}
+
+template <class C>
+__device__ __forceinline__ fe<C> operator*(const fe<C>& a, const fe<C>& b) {
+  return fe_mul_call<C>(a, b);
 }
 
 template <class C>

@@ -105,12 +105,12 @@ __global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const 
       }
       fr_t a, b;
       if (DIT) {
-        v = v * w;
+        v = fe_mul_inline(v, w);
         a = u + v;
         b = u - v;
       } else {
         a = u + v;
-        b = (u - v) * w;
+        b = fe_mul_inline(u - v, w);
       }
 #pragma unroll
       for (int q = 0; q < 8; q++) {

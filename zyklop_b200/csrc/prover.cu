@@ -67,7 +67,8 @@ __global__ void __launch_bounds__(256) k_spmv(SpmvArgs a, const fr_t* __restrict
   const int m = blockIdx.y;
   const uint32_t b = a.row[m][i], e = a.row[m][i + 1];
   fr_t acc = fe_zero<FrCfg>();
-  for (uint32_t k = b; k < e; k++) acc = acc + fe_ldg<FrCfg>(a.val[m], k) * fe_ldg<FrCfg>(w, a.sig[m][k]);
+  for (uint32_t k = b; k < e; k++)
+    acc = acc + fe_mul_inline(fe_ldg<FrCfg>(a.val[m], k), fe_ldg<FrCfg>(w, a.sig[m][k]));
   fe_store(a.out[m], i, acc);
 }
 
