@@ -197,6 +197,47 @@ int zk_prove(zk_circuit* c, const uint64_t* h_witness, size_t n_witness, const u
              const uint64_t* s, uint64_t* proof);
 int zk_prove_device(zk_circuit* c, const uint64_t* d_witness, size_t n_witness, const uint64_t* r,
                     const uint64_t* s, uint64_t* proof);
+/* Proves `count` jobs: circuits[i] (all loaded on `ctx`) with witnesses[i]
+ * (n_witness[i] values; host memory, or device memory if on_device != 0),
+ * writing proofs + 32 * i.  Up to `inflight` (1..16) proofs are on the GPU at
+ * once, each on its own workspace and streams, so one proof's serial tail
+ * (window combination, blinding) overlaps the next proofs' kernels.  r, s:
+ * count x 4 u64 blinding scalars, or both NULL.  Every proof equals the one
+ * zk_prove gives for the same job.  No reference counterpart (the reference
+ * proves one file pair per process). */
+int zk_prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* circuits,
+                   const uint64_t* const* witnesses, const size_t* n_witness, int on_device,
+                   const uint64_t* r, const uint64_t* s, uint64_t* proofs, int inflight);
+/* When on, each workspace captures a proof's device pipeline (about 60
+ * kernels and copies across 5 streams) into a CUDA graph the first time it
+ * proves a circuit and replays it afterwards.  Results are unchanged. */
+int zk_ctx_set_graphs(zk_ctx* ctx, int on);
+
+/* Proof server: continuous batching over resident circuits.  A worker thread
+ * keeps up to max_inflight proofs on the GPU, each in its own workspace with
+ * its own streams; queued requests are admitted in arrival order as soon as a
+ * workspace is free and the device has room for its buffers plus
+ * reserve_bytes (admission by free memory), so a request that arrives while
+ * others run overlaps with them.  Each proof equals the one zk_prove gives
+ * for the same job.  The witness buffer and the circuit must stay valid until
+ * zk_server_wait returns for that ticket.  No reference counterpart (the
+ * reference proves one file pair per process). */
+typedef struct zk_server zk_server;
+int zk_server_create(zk_ctx* ctx, int max_inflight, size_t reserve_bytes, zk_server** out);
+/* Queues one proof; r and s (4 u64 each) are blinding scalars or both NULL. */
+int zk_server_submit(zk_server* srv, zk_circuit* c, const uint64_t* h_witness, size_t n_witness,
+                     const uint64_t* r, const uint64_t* s, uint64_t* ticket);
+/* Waits for a ticket (timeout_ms < 0: no limit; ZK_ETIMEOUT when it runs out,
+ * the ticket stays valid), writes the 32-u64 proof and the time from submit
+ * to completion.  A failed proof returns its error code; the ticket is then
+ * released either way. */
+int zk_server_wait(zk_server* srv, uint64_t ticket, int timeout_ms, uint64_t* proof,
+                   double* latency_ms);
+int zk_server_stats(zk_server* srv, uint64_t* completed, uint64_t* failed,
+                    uint64_t* peak_inflight, uint64_t* admission_waits);
+/* Finishes every queued proof, then stops the worker and frees the server. */
+int zk_server_destroy(zk_server* srv);
+
 /* Unblinded proof that also copies out A.w, B.w (Montgomery, domain x 4 u64)
  * and h (canonical, domain x 4 u64) into host buffers (any may be NULL).
  * For checking the pipeline's intermediates. */

@@ -235,3 +235,125 @@ def test_malformed_inputs_are_status_codes(api, files, tmp_path):
     assert e.value.code == 6  # ZK_EWITNESS
     # the context stays usable after the failures
     assert np.array_equal(c.prove(api.read_wtns(w)), api.prove_files(z, w))
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+@pytest.mark.parametrize("inflight", [1, 3])
+def test_batch_matches_single_proofs(api, oracle, files, graphs, inflight):
+    """A batch over mixed circuits gives, job for job, the proofs zk_prove gives."""
+    names = ["u10", "c10", "u16", "u10", "c10", "u16", "c10"]
+    circ = {nm: api.Circuit(files[nm][0]) for nm in set(names)}
+    wits = {nm: api.read_wtns(files[nm][1]) for nm in set(names)}
+    single = {nm: circ[nm].prove(wits[nm]) for nm in circ}
+    try:
+        api.set_graphs(graphs)
+        proofs = api.prove_batch([circ[nm] for nm in names], [wits[nm] for nm in names],
+                                 inflight=inflight)
+        for k, nm in enumerate(names):
+            assert np.array_equal(proofs[k], single[nm]), (k, nm)
+        # blinded batch equals the oracle's blinded proofs
+        rs = [11 + k for k in range(3)]
+        ss = [101 + k for k in range(3)]
+        sub = names[:3]
+        bp = api.prove_batch([circ[nm] for nm in sub], [wits[nm] for nm in sub],
+                             inflight=inflight, rs=rs, ss=ss)
+        for k, nm in enumerate(sub):
+            z, w = files[nm]
+            assert np.array_equal(bp[k], oracle.prove(blob(z), blob(w), r=rs[k], s=ss[k]))
+        # a second replay of the captured graphs gives the same proofs
+        again = api.prove_batch([circ[nm] for nm in names], [wits[nm] for nm in names],
+                                inflight=inflight)
+        assert np.array_equal(again, proofs)
+    finally:
+        api.set_graphs(False)
+
+
+def test_batch_rejects_short_witness_and_recovers(api, files):
+    from zyklop_b200 import ZkError
+    z, w = files["u10"]
+    c = api.Circuit(z)
+    wit = api.read_wtns(w)
+    with pytest.raises(ZkError) as e:
+        api.prove_batch([c, c], [wit, wit[:5]])
+    assert e.value.code == 6
+    assert np.array_equal(api.prove_batch([c], [wit])[0], c.prove(wit))
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_server_results_same_alone_and_in_mix(api, oracle, files, graphs):
+    """Proofs from the continuous-batching server equal the proofs each job
+    gives alone, whatever else is in flight beside it."""
+    import threading
+    names = ["u16", "u10", "c10", "u10", "u16", "c10", "u10", "u16"]
+    circ = {nm: api.Circuit(files[nm][0]) for nm in set(names)}
+    wits = {nm: api.read_wtns(files[nm][1]) for nm in set(names)}
+    alone = {nm: circ[nm].prove(wits[nm]) for nm in circ}
+    blind = {2: (7, 9), 5: (123456789, 987654321)}
+    try:
+        api.set_graphs(graphs)
+        with api.Server(max_inflight=3) as srv:
+            tickets = []
+            for k, nm in enumerate(names):
+                r, s = blind.get(k, (None, None))
+                tickets.append(srv.submit(circ[nm], wits[nm], r=r, s=s))
+            # more requests from other host threads while those run
+            extra = {}
+
+            def client(tid):
+                extra[tid] = [srv.submit(circ[nm], wits[nm]) for nm in ("u10", "u16")]
+
+            th = [threading.Thread(target=client, args=(t,)) for t in range(3)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            for k, nm in enumerate(names):
+                proof, lat = srv.wait(tickets[k])
+                assert lat > 0
+                if k in blind:
+                    z, w = files[nm]
+                    r, s = blind[k]
+                    assert np.array_equal(proof, oracle.prove(blob(z), blob(w), r=r, s=s)), k
+                else:
+                    assert np.array_equal(proof, alone[nm]), (k, nm)
+            for tid, ts in extra.items():
+                for t, nm in zip(ts, ("u10", "u16")):
+                    assert np.array_equal(srv.wait(t)[0], alone[nm]), (tid, nm)
+            st = srv.stats()
+            assert st["completed"] == len(names) + 6 and st["failed"] == 0
+            assert 1 <= st["peak_inflight"] <= 3
+    finally:
+        api.set_graphs(False)
+
+
+def test_server_admission_by_free_memory(api, files):
+    """With a reserve larger than the device, a request is admitted only when
+    nothing else runs: one proof in flight at a time, all of them correct."""
+    z, w = files["u16"]
+    c = api.Circuit(z)
+    wit = api.read_wtns(w)
+    ref = c.prove(wit)
+    with api.Server(max_inflight=4, reserve_bytes=1 << 50) as srv:
+        ts = [srv.submit(c, wit) for _ in range(4)]
+        for t in ts:
+            assert np.array_equal(srv.wait(t)[0], ref)
+        st = srv.stats()
+    assert st["peak_inflight"] == 1 and st["completed"] == 4
+
+
+def test_server_errors(api, files):
+    from zyklop_b200 import ZkError
+    z, w = files["u10"]
+    c = api.Circuit(z)
+    wit = api.read_wtns(w)
+    with api.Server(max_inflight=2) as srv:
+        bad = srv.submit(c, wit[:5])
+        good = srv.submit(c, wit)
+        with pytest.raises(ZkError) as e:
+            srv.wait(bad)
+        assert e.value.code == 6
+        assert np.array_equal(srv.wait(good)[0], c.prove(wit))
+        with pytest.raises(ZkError) as e:
+            srv.wait(good)  # released
+        assert e.value.code == 1
+        assert srv.stats()["failed"] == 1

@@ -69,6 +69,18 @@ SIGNATURES = {
     "zk_prove_intermediates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               u64p]),
+    "zk_prove_batch": (ctypes.c_int, [ctypes.c_void_p, sz, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, u64p, ctypes.c_int]),
+    "zk_ctx_set_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "zk_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, sz,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "zk_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, u64p, sz, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "zk_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, u64p,
+                                      ctypes.POINTER(ctypes.c_double)]),
+    "zk_server_stats": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_uint64)] * 4),
+    "zk_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_groth16_prove_files": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
                                               u64p]),
     "zk_groth16_prove_mem": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz, ctypes.c_void_p,

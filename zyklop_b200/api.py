@@ -9,7 +9,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import ZkError, check, lib
 
 FP, FR = 0, 1
 OPS = {"mul": 0, "add": 1, "sub": 2, "sqr": 3, "neg": 4, "inv": 5, "encode": 6, "decode": 7}
@@ -264,3 +264,98 @@ class MsmTable:
             self.close()
         except Exception:
             pass
+
+
+def prove_batch(circuits, witnesses, inflight=3, rs=None, ss=None, on_device=False, ctx=None):
+    """Prove many jobs with several proofs in flight (zk_prove_batch).
+
+    circuits: Circuit objects (same context); witnesses: (n, 4) uint64 arrays
+    (or device tensors with on_device=True).  rs / ss: optional lists of ints.
+    Returns a (count, 32) uint64 array of proofs."""
+    count = len(circuits)
+    handles = (ctypes.c_void_p * count)(*[c.handle.value for c in circuits])
+    if on_device:
+        wptrs = [w.data_ptr() for w in witnesses]
+        ns = [w.numel() // 4 for w in witnesses]
+    else:
+        ws = [np.ascontiguousarray(w, dtype=np.uint64).reshape(-1, 4) for w in witnesses]
+        wptrs = [w.ctypes.data for w in ws]
+        ns = [w.shape[0] for w in ws]
+    wp = (ctypes.c_void_p * count)(*wptrs)
+    nw = (ctypes.c_size_t * count)(*ns)
+    proofs = np.zeros((count, 32), dtype=np.uint64)
+    rb = sb = None
+    if rs is not None:
+        rb = np.array([[(x >> (64 * i)) & (2**64 - 1) for i in range(4)] for x in rs], np.uint64)
+        sb = np.array([[(x >> (64 * i)) & (2**64 - 1) for i in range(4)] for x in ss], np.uint64)
+    check(lib().zk_prove_batch(ctx, count, handles, wp, nw, 1 if on_device else 0,
+                               rb.ctypes.data_as(ctypes.c_void_p) if rb is not None else None,
+                               sb.ctypes.data_as(ctypes.c_void_p) if sb is not None else None,
+                               proofs.ctypes.data_as(_u64p), inflight))
+    return proofs
+
+
+def set_graphs(on, ctx=None):
+    check(lib().zk_ctx_set_graphs(ctx, 1 if on else 0))
+
+
+def _limbs(x):
+    return np.array([(x >> (64 * i)) & (2**64 - 1) for i in range(4)], np.uint64)
+
+
+class Server:
+    """Continuous-batching proof server (zk_server_*).
+
+    submit() queues a proof and returns a ticket at once; wait(ticket) returns
+    (proof, latency_ms).  The server keeps each submitted witness alive until
+    its ticket is waited for."""
+
+    def __init__(self, max_inflight=4, reserve_bytes=0, ctx=None):
+        h = ctypes.c_void_p()
+        check(lib().zk_server_create(ctx, max_inflight, reserve_bytes, ctypes.byref(h)))
+        self.handle = h
+        self._keep = {}
+
+    def submit(self, circuit, witness, r=None, s=None):
+        w = np.ascontiguousarray(witness, dtype=np.uint64).reshape(-1, 4)
+        rb = _limbs(r) if r is not None else None
+        sb = _limbs(s) if s is not None else None
+        t = ctypes.c_uint64()
+        check(lib().zk_server_submit(self.handle, circuit.handle, w.ctypes.data_as(_u64p),
+                                     w.shape[0],
+                                     rb.ctypes.data_as(ctypes.c_void_p) if rb is not None else None,
+                                     sb.ctypes.data_as(ctypes.c_void_p) if sb is not None else None,
+                                     ctypes.byref(t)))
+        self._keep[t.value] = w
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        proof = np.zeros(32, dtype=np.uint64)
+        lat = ctypes.c_double()
+        try:
+            check(lib().zk_server_wait(self.handle, ticket, timeout_ms, proof.ctypes.data_as(_u64p),
+                                       ctypes.byref(lat)))
+        except ZkError as e:
+            if e.code != 7:  # ZK_ETIMEOUT keeps the ticket
+                self._keep.pop(ticket, None)
+            raise
+        self._keep.pop(ticket, None)
+        return proof, lat.value
+
+    def stats(self):
+        v = [ctypes.c_uint64() for _ in range(4)]
+        check(lib().zk_server_stats(self.handle, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("completed", "failed", "peak_inflight", "admission_waits"),
+                        [x.value for x in v]))
+
+    def close(self):
+        if self.handle is not None and self.handle.value:
+            check(lib().zk_server_destroy(self.handle))
+            self.handle = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -167,6 +167,25 @@ int zk_prove_intermediates(zk_circuit* c, const uint64_t* h_witness, size_t n_wi
   ZK_API_END
 }
 
+int zk_prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* circuits,
+                   const uint64_t* const* witnesses, const size_t* n_witness, int on_device,
+                   const uint64_t* r, const uint64_t* s, uint64_t* proofs, int inflight) {
+  ZK_API_BEGIN
+  ZK_REQUIRE((r == nullptr) == (s == nullptr), ZK_EINVAL, "zk_prove_batch: give both r and s or neither");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  prove_batch(ctx, count, circuits, witnesses, n_witness, on_device != 0, r, s, proofs, inflight);
+  ZK_API_END
+}
+
+int zk_ctx_set_graphs(zk_ctx* ctx, int on) {
+  ZK_API_BEGIN
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->use_graphs = on != 0;
+  ZK_API_END
+}
+
 int zk_groth16_prove_mem(zk_ctx* ctx, const uint8_t* zkey, size_t zkey_len, const uint8_t* wtns,
                          size_t wtns_len, uint64_t* proof) {
   ZK_API_BEGIN

@@ -2,7 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <mutex>
+#include <vector>
 
 #include "msm.hpp"
 #include "ntt.hpp"
@@ -11,18 +13,40 @@
 
 namespace zk {
 
-// Buffers and streams of one in-flight proof (reused across proofs).
+// Largest MSM result copied to the host: 2 x 64 windows of G2 XYZZ points.
+constexpr size_t kMaxWindowBytes = 2 * 64 * 256;
+
+// Buffers and streams of one in-flight proof (reused across proofs).  A
+// context has one for single proofs and a pool for batches (a proof server
+// has its own); each can hold captured graphs of its device pipeline.
 struct ProveWs {
   static constexpr int kStreams = 5;  // 0: witness/SpMV/H/MSM_H, 1: A, 2: B2, 3: C, 4: B1
   bool ready = false;
   int nstreams = kStreams;
   cudaStream_t st[kStreams] = {};
-  cudaEvent_t ev_we = nullptr, ev_begin = nullptr;
+  cudaEvent_t ev_we = nullptr, ev_begin = nullptr, ev_all = nullptr;
   cudaEvent_t ev_done[kStreams] = {};
   DeviceBuffer we, aw, bw, cw, h;
   DeviceBuffer msm[kStreams];
   PinnedBuffer win[kStreams];
+  MsmResult res[kStreams];
+  // captured pipelines, one per (circuit, blinding); all are dropped when a
+  // buffer they point into is reallocated
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t circuit = 0;  // circuit id the graph was captured for
+    bool blind = false;
+    int ntt_lmax = 0;  // twiddle table the graph reads
+    MsmConfig cfg[2];  // G1 / G2 MSM settings captured
+    int tab_c[2] = {0, 0};  // fixed-base table windows captured (0: windowed)
+    uint64_t kernels = 0;
+    MsmResult res[kStreams];  // where and how the graph leaves each MSM's windows
+  };
+  static constexpr size_t kMaxGraphs = 8;
+  std::vector<Graph> graphs;
   void init();
+  void drop_graph();
+  cudaEvent_t ev_begin_pool() { init(); return ev_begin; }
   ~ProveWs();
 };
 
@@ -37,6 +61,8 @@ struct zk_ctx {
   zk::DeviceBuffer msm_scratch;
   zk::MsmConfig msm_cfg[2];
   zk::ProveWs ws;
+  std::vector<std::unique_ptr<zk::ProveWs>> pool;  // batch workspaces
+  bool use_graphs = false;  // replay captured per-circuit proof graphs
   zk::Stager stager;
   zk::Profiler prof;
   bool profiling = false;

@@ -15,10 +15,13 @@
 //                   thread's work (skewed scalars stay balanced); buckets that
 //                   cross thread ranges leave partial sums that further levels
 //                   of the same kernel combine;
-//   5. msm_bucket_reduce / msm_window_reduce
-//                   sum_b (b+1) S_b per window from chunked running sums;
-//   6. host         Horner over windows (latency-bound, done on one CPU core)
-//                   and affine conversion.
+//   5. msm_reduce_l1 / msm_reduce_blk
+//                   sum_b (b+1) S_b per window: running sums over chunks of
+//                   buckets, then block-parallel passes (suffix scan + tree
+//                   sum over 128 partial pairs each) down to one (U, A) pair
+//                   per window;
+//   6. host         A + 2^log_span U, Horner over windows (latency-bound,
+//                   done on one CPU core) and affine conversion.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -34,6 +37,9 @@ struct MsmConfig {
   int k0 = 64;        // sorted records per thread in the first accumulation level
   int k1 = 16;        // partial records per thread in later levels
   int chunk = 16;     // buckets per thread in the bucket reduction
+  bool operator==(const MsmConfig& o) const {
+    return c == o.c && k0 == o.k0 && k1 == o.k1 && chunk == o.chunk;
+  }
 };
 
 // Affine input points: x of point i at x + i*stride coordinates, y likewise.

@@ -1,6 +1,7 @@
 // Groth16 prover on sm_100a (see prover.hpp).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -110,6 +111,7 @@ P mul(const P& p, const uint64_t* k) {
 
 void ProveWs::init() {
   if (ready) return;
+  ZK_CUDA(cudaEventCreateWithFlags(&ev_all, cudaEventDisableTiming));
   // ZYKLOP_PROVE_STREAMS=1 runs a proof's MSMs back to back on one stream
   // (a tuning knob: concurrent MSMs share L2 and the SMs)
   if (const char* e = getenv("ZYKLOP_PROVE_STREAMS")) {
@@ -134,12 +136,15 @@ ProveWs::~ProveWs() {
   }
   cudaEventDestroy(ev_we);
   cudaEventDestroy(ev_begin);
+  cudaEventDestroy(ev_all);
+  drop_graph();
 }
 
 zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
   const ZkeyView z = parse_zkey(f);
   std::unique_ptr<zk_circuit> c(new zk_circuit());
   c->ctx = ctx;
+  c->id = next_circuit_id();
   c->m1 = z.n_vars;
   c->l = z.n_public;
   c->n = z.domain;
@@ -253,22 +258,14 @@ void circuit_precompute(zk_circuit* c, int c_g1, int c_g2) {
   c->tab_c[1] = g2c;
 }
 
-void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_device,
-           const uint64_t* r, const uint64_t* s, uint64_t proof[32], ProveIntermediates* dbg) {
+namespace {
+
+std::atomic<uint64_t> g_circuit_ids{1};
+
+// MSM scratch bytes of each of a proof's MSMs (indexed like ProveWs::msm).
+void ws_scratch_needs(zk_circuit* c, bool blind, size_t need[ProveWs::kStreams]) {
   zk_ctx* ctx = c->ctx;
-  ZK_REQUIRE(n_witness >= c->m1, ZK_EWITNESS, "witness has fewer values than the circuit's nVars");
-  ZK_REQUIRE(witness, ZK_EINVAL, "NULL witness");
-  const bool blind = r && s;
-  ZK_REQUIRE(!blind || c->has_b1, ZK_EFORMAT, "blinding needs zkey section 6 (B1 points)");
-  ProveWs& ws = ctx->ws;
-  ws.init();
   const size_t m1 = c->m1, n = c->n, l = c->l, nc = m1 - l - 1;
-  ws.we.ensure(32 * (m1 + 1));
-  ws.aw.ensure(32 * n);
-  ws.bw.ensure(32 * n);
-  ws.cw.ensure(32 * n);
-  ws.h.ensure(32 * n);
-  ctx->ntt.ensure(c->log_n, ws.st[0]);
   const MsmConfig& c1 = ctx->msm_cfg[0];
   const MsmConfig& c2 = ctx->msm_cfg[1];
   const bool fixed = c->tab_c[0] != 0;
@@ -276,49 +273,85 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
     return fixed ? msm_scratch_bytes_fixed(cnt, g2, c->tab_c[g2 ? 1 : 0], g2 ? c2 : c1)
                  : msm_scratch_bytes(cnt, g2, g2 ? c2 : c1);
   };
-  const size_t need[ProveWs::kStreams] = {scratch(n, false), scratch(m1 + 1, false),
-                                          scratch(m1 + 1, true), scratch(nc, false),
-                                          blind ? scratch(m1 + 1, false) : 0};
-  for (int i = 0; i < ProveWs::kStreams; i++)
-    if (need[i]) {
-      if (ws.msm[i].cap < need[i]) ZK_CUDA(cudaStreamSynchronize(ws.st[i]));
-      ws.msm[i].ensure(need[i]);
-    }
+  need[0] = scratch(n, false);
+  need[1] = scratch(m1 + 1, false);
+  need[2] = scratch(m1 + 1, true);
+  need[3] = scratch(nc, false);
+  need[4] = blind ? scratch(m1 + 1, false) : 0;
+}
 
-  // the proof starts after prior work on the context stream and ends before
-  // later work on it, so callers can bracket it with events on that stream
-  ZK_CUDA(cudaEventRecord(ws.ev_begin, ctx->stream));
-  for (int i = 0; i < ProveWs::kStreams; i++) ZK_CUDA(cudaStreamWaitEvent(ws.st[i], ws.ev_begin, 0));
+// Sizes the workspace for this circuit (buffers, MSM scratch, result copies).
+void ws_prepare(zk_circuit* c, ProveWs& ws, bool blind) {
+  zk_ctx* ctx = c->ctx;
+  ws.init();
+  const size_t m1 = c->m1, n = c->n;
+  size_t need[ProveWs::kStreams];
+  ws_scratch_needs(c, blind, need);
+  const bool grow = ws.we.cap < 32 * (m1 + 1) || ws.aw.cap < 32 * n ||
+                    [&] {
+                      for (int i = 0; i < ProveWs::kStreams; i++)
+                        if (ws.msm[i].cap < need[i]) return true;
+                      return false;
+                    }();
+  if (grow) {
+    for (int i = 0; i < ProveWs::kStreams; i++) ZK_CUDA(cudaStreamSynchronize(ws.st[i]));
+    ws.drop_graph();  // captured addresses change
+  }
+  ws.we.ensure(32 * (m1 + 1));
+  ws.aw.ensure(32 * n);
+  ws.bw.ensure(32 * n);
+  ws.cw.ensure(32 * n);
+  ws.h.ensure(32 * n);
+  for (int i = 0; i < ProveWs::kStreams; i++) {
+    if (need[i]) ws.msm[i].ensure(need[i]);
+    ws.win[i].ensure(kMaxWindowBytes);
+  }
+  ctx->ntt.ensure(c->log_n, ws.st[0]);
+}
 
-  // 1. witness: we = [1 || w_0 .. w_{m1-1}] (src/groth16.cu:1316-1326)
+// Witness into we = [1 || w_0 .. w_{m1-1}] on stream 0 (src/groth16.cu:1316-1326).
+void ws_stage(zk_circuit* c, ProveWs& ws, const uint64_t* witness, bool on_device,
+              Stager& stager) {
   cudaStream_t s0 = ws.st[0];
   uint64_t* we = ws.we.as<uint64_t>();
   ZK_CUDA(cudaMemsetAsync(we, 0, 32, s0));
   ZK_CUDA(cudaMemsetAsync(we, 1, 1, s0));
   if (on_device)
-    ZK_CUDA(cudaMemcpyAsync(we + 4, witness, 32 * m1, cudaMemcpyDeviceToDevice, s0));
+    ZK_CUDA(cudaMemcpyAsync(we + 4, witness, 32 * (size_t)c->m1, cudaMemcpyDeviceToDevice, s0));
   else
-    ctx->stager.upload(we + 4, witness, 32 * m1, s0);
-  ZK_CUDA(cudaEventRecord(ws.ev_we, s0));
+    stager.upload(we + 4, witness, 32 * (size_t)c->m1, s0);
+}
 
-  // 2. MSMs that only need the witness, on their own streams
-  MsmResult res[ProveWs::kStreams];
+// The device part of a proof, from the staged witness to the MSM results in
+// pinned host memory.  It begins and ends on stream 0 (other streams fork
+// from and join back to it), issues no synchronizing call, and can therefore
+// be captured into a CUDA graph.
+void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg) {
+  zk_ctx* ctx = c->ctx;
+  const size_t m1 = c->m1, n = c->n, l = c->l, nc = m1 - l - 1;
+  const MsmConfig& c1 = ctx->msm_cfg[0];
+  const MsmConfig& c2 = ctx->msm_cfg[1];
+  const bool fixed = c->tab_c[0] != 0;
+  cudaStream_t s0 = ws.st[0];
+  uint64_t* we = ws.we.as<uint64_t>();
+  ZK_CUDA(cudaEventRecord(ws.ev_we, s0));
   auto launch = [&](int i, bool g2, const DeviceBuffer& pts, const DeviceBuffer& tab,
                     const uint64_t* sc, size_t cnt) {
     const int si = i % ws.nstreams;
     cudaStream_t st = ws.st[si];
     if (si) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
     if (fixed)
-      res[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
-                                 ws.msm[i].cap, g2 ? c2 : c1, st);
+      ws.res[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
+                                    ws.msm[i].cap, g2 ? c2 : c1, st);
     else if (g2)
-      res[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap, c2,
-                              st);
+      ws.res[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr,
+                                 ws.msm[i].cap, c2, st);
     else
-      res[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap,
-                              c1, st);
-    ws.win[i].ensure(res[i].bytes);
-    ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, res[i].d_data, res[i].bytes, cudaMemcpyDeviceToHost, st));
+      ws.res[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr,
+                                 ws.msm[i].cap, c1, st);
+    ZK_REQUIRE(ws.res[i].bytes <= kMaxWindowBytes, ZK_EINTERNAL, "prove: MSM result too large");
+    ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, ws.res[i].d_data, ws.res[i].bytes,
+                            cudaMemcpyDeviceToHost, st));
     ZK_CUDA(cudaEventRecord(ws.ev_done[i], st));
   };
   launch(1, false, c->pts_a, c->tab_a, we, m1 + 1);
@@ -326,7 +359,6 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   launch(3, false, c->pts_c, c->tab_c_pts, we + 4 * (l + 2), nc);
   if (blind) launch(4, false, c->pts_b1, c->tab_b1, we, m1 + 1);
 
-  // 3. SpMV -> H -> MSM_H on stream 0
   SpmvArgs sa;
   for (int m = 0; m < 2; m++) {
     sa.row[m] = c->row[m].as<uint32_t>();
@@ -336,38 +368,91 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   sa.out[0] = ws.aw.as<fr_t>();
   sa.out[1] = ws.bw.as<fr_t>();
   {
-  ProfScope prof(kProfSpmv, (double)c->n_coefs, s0);
-  k_spmv<<<dim3(blocks(n, 256), 2), 256, 0, s0>>>(sa, reinterpret_cast<const fr_t*>(we + 4),
-                                                  (uint32_t)n);
-  ZK_LAUNCHED();
+    ProfScope prof(kProfSpmv, (double)c->n_coefs, s0);
+    k_spmv<<<dim3(blocks(n, 256), 2), 256, 0, s0>>>(sa, reinterpret_cast<const fr_t*>(we + 4),
+                                                    (uint32_t)n);
+    ZK_LAUNCHED();
   }
-  ZK_CHECK_LAUNCH();
   if (dbg && (dbg->aw || dbg->bw)) {
     if (dbg->aw) ZK_CUDA(cudaMemcpyAsync(dbg->aw, ws.aw.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
     if (dbg->bw) ZK_CUDA(cudaMemcpyAsync(dbg->bw, ws.bw.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
-    ZK_CUDA(cudaStreamSynchronize(s0));
   }
   hpoly(ctx->ntt, ws.aw.as<uint64_t>(), ws.bw.as<uint64_t>(), ws.cw.as<uint64_t>(), c->log_n,
         ws.h.as<uint64_t>(), s0);
-  if (dbg && dbg->h) {
-    ZK_CUDA(cudaMemcpyAsync(dbg->h, ws.h.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
-    ZK_CUDA(cudaStreamSynchronize(s0));
-  }
+  if (dbg && dbg->h) ZK_CUDA(cudaMemcpyAsync(dbg->h, ws.h.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
   launch(0, false, c->pts_h, c->tab_h, ws.h.as<uint64_t>(), n);
+  for (int i = 1; i < (blind ? 5 : 4); i++) ZK_CUDA(cudaStreamWaitEvent(s0, ws.ev_done[i], 0));
+}
 
-  // 4. host: combine the window sums, assemble the proof
-  const int used = blind ? 5 : 4;
-  for (int i = 0; i < used; i++) ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_done[i], 0));
-  for (int i = 0; i < used; i++) ZK_CUDA(cudaEventSynchronize(ws.ev_done[i]));
+// Runs the pipeline directly or as a replay of its captured graph.
+void ws_launch(zk_circuit* c, ProveWs& ws, bool blind, bool use_graph, ProveIntermediates* dbg) {
+  if (!use_graph || dbg) {
+    ws_pipeline(c, ws, blind, dbg);
+    return;
+  }
+  const zk_ctx* ctx = c->ctx;
+  const int lmax = ctx->ntt.lmax;
+  ProveWs::Graph* gr = nullptr;
+  for (ProveWs::Graph& x : ws.graphs)
+    if (x.circuit == c->id && x.blind == blind && x.ntt_lmax == lmax &&
+        x.cfg[0] == ctx->msm_cfg[0] && x.cfg[1] == ctx->msm_cfg[1] && x.tab_c[0] == c->tab_c[0] &&
+        x.tab_c[1] == c->tab_c[1])
+      gr = &x;
+  if (!gr) {
+    if (ws.graphs.size() >= ProveWs::kMaxGraphs) {
+      cudaGraphExecDestroy(ws.graphs.front().exec);
+      ws.graphs.erase(ws.graphs.begin());
+    }
+    Profiler* saved = current_profiler();
+    set_current_profiler(nullptr);  // no timing events inside a capture
+    const uint64_t l0 = launch_count();
+    cudaGraph_t g = nullptr;
+    ZK_CUDA(cudaStreamBeginCapture(ws.st[0], cudaStreamCaptureModeThreadLocal));
+    try {
+      ws_pipeline(c, ws, blind, nullptr);
+    } catch (...) {
+      cudaStreamEndCapture(ws.st[0], &g);
+      if (g) cudaGraphDestroy(g);
+      set_current_profiler(saved);
+      throw;
+    }
+    ZK_CUDA(cudaStreamEndCapture(ws.st[0], &g));
+    set_current_profiler(saved);
+    ProveWs::Graph x;
+    const cudaError_t e = cudaGraphInstantiate(&x.exec, g, 0);
+    cudaGraphDestroy(g);
+    ZK_CUDA(e);
+    x.kernels = launch_count() - l0;
+    x.circuit = c->id;
+    x.blind = blind;
+    x.ntt_lmax = lmax;
+    x.cfg[0] = ctx->msm_cfg[0];
+    x.cfg[1] = ctx->msm_cfg[1];
+    x.tab_c[0] = c->tab_c[0];
+    x.tab_c[1] = c->tab_c[1];
+    for (int i = 0; i < ProveWs::kStreams; i++) x.res[i] = ws.res[i];
+    ws.graphs.push_back(x);
+    gr = &ws.graphs.back();
+  }
+  // the host combine reads these; another circuit's run may have replaced them
+  for (int i = 0; i < ProveWs::kStreams; i++) ws.res[i] = gr->res[i];
+  ZK_CUDA(cudaGraphLaunch(gr->exec, ws.st[0]));
+  count_launch((int)gr->kernels);
+}
+
+// Waits for the device work, combines the MSM results, applies blinding.
+void ws_finish(zk_circuit* c, ProveWs& ws, bool blind, const uint64_t* r, const uint64_t* s,
+               uint64_t proof[32]) {
+  ZK_CUDA(cudaEventSynchronize(ws.ev_all));
   uint64_t pa[8], pb[16], pc[8], ph[8], pb1[8];
-  msm_g1_combine(ws.win[1].ptr, res[1], pa);
-  msm_g2_combine(ws.win[2].ptr, res[2], pb);
-  msm_g1_combine(ws.win[3].ptr, res[3], pc);
-  msm_g1_combine(ws.win[0].ptr, res[0], ph);
+  msm_g1_combine(ws.win[1].ptr, ws.res[1], pa);
+  msm_g2_combine(ws.win[2].ptr, ws.res[2], pb);
+  msm_g1_combine(ws.win[3].ptr, ws.res[3], pc);
+  msm_g1_combine(ws.win[0].ptr, ws.res[0], ph);
   G1 A = g1_aff(pa), Cc = g1_aff(pc).add(g1_aff(ph));
   G2 B = g2_aff(pb);
   if (blind) {
-    msm_g1_combine(ws.win[4].ptr, res[4], pb1);
+    msm_g1_combine(ws.win[4].ptr, ws.res[4], pb1);
     const G1 d1 = g1_aff(c->delta1);
     A = A.add(mul(d1, r));
     B = B.add(mul(g2_aff(c->delta2), s));
@@ -379,6 +464,107 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   g1_out(A, proof);
   g2_out(B, proof + 8);
   g1_out(Cc, proof + 24);
+}
+
+void check_job(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool blind) {
+  ZK_REQUIRE(c, ZK_EINVAL, "NULL circuit");
+  ZK_REQUIRE(witness, ZK_EINVAL, "NULL witness");
+  ZK_REQUIRE(n_witness >= c->m1, ZK_EWITNESS, "witness has fewer values than the circuit's nVars");
+  ZK_REQUIRE(!blind || c->has_b1, ZK_EFORMAT, "blinding needs zkey section 6 (B1 points)");
+}
+
+}  // namespace
+
+// Device bytes that preparing ws for this circuit would newly allocate (the
+// proof server admits a request only when that much memory is free).
+size_t ws_bytes_needed(zk_circuit* c, const ProveWs& ws, bool blind) {
+  size_t need[ProveWs::kStreams];
+  ws_scratch_needs(c, blind, need);
+  const size_t m1 = c->m1, n = c->n;
+  auto grow = [](const DeviceBuffer& b, size_t want) { return b.cap < want ? want : size_t(0); };
+  size_t total = grow(ws.we, 32 * (m1 + 1)) + grow(ws.aw, 32 * n) + grow(ws.bw, 32 * n) +
+                 grow(ws.cw, 32 * n) + grow(ws.h, 32 * n);
+  for (int i = 0; i < ProveWs::kStreams; i++) total += grow(ws.msm[i], need[i]);
+  if (c->ctx->ntt.lmax < c->log_n) total += 2 * 16 * n;  // twiddle tables of 2^(log_n-1)
+  return total;
+}
+
+// Starts a proof from a host witness on ws's streams without waiting for it.
+void ws_submit(zk_circuit* c, ProveWs& ws, const uint64_t* witness, bool blind, Stager& stager) {
+  ws_prepare(c, ws, blind);
+  ws_stage(c, ws, witness, false, stager);
+  ws_launch(c, ws, blind, c->ctx->use_graphs, nullptr);
+  ZK_CUDA(cudaEventRecord(ws.ev_all, ws.st[0]));
+}
+
+// True once the submitted proof's device work has ended (or failed).
+bool ws_ready(ProveWs& ws) { return cudaEventQuery(ws.ev_all) != cudaErrorNotReady; }
+
+// Combines a finished proof (raises the device error of a failed one).
+void ws_collect(zk_circuit* c, ProveWs& ws, bool blind, const uint64_t* r, const uint64_t* s,
+                uint64_t proof[32]) {
+  ws_finish(c, ws, blind, r, s, proof);
+}
+
+uint64_t next_circuit_id() { return g_circuit_ids.fetch_add(1); }
+
+void ProveWs::drop_graph() {
+  for (Graph& g : graphs) cudaGraphExecDestroy(g.exec);
+  graphs.clear();
+}
+
+void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_device,
+           const uint64_t* r, const uint64_t* s, uint64_t proof[32], ProveIntermediates* dbg) {
+  const bool blind = r && s;
+  check_job(c, witness, n_witness, blind);
+  zk_ctx* ctx = c->ctx;
+  ProveWs& ws = ctx->ws;
+  ws_prepare(c, ws, blind);
+  // the proof starts after prior work on the context stream and ends before
+  // later work on it, so callers can bracket it with events on that stream
+  ZK_CUDA(cudaEventRecord(ws.ev_begin, ctx->stream));
+  ZK_CUDA(cudaStreamWaitEvent(ws.st[0], ws.ev_begin, 0));
+  ws_stage(c, ws, witness, on_device, ctx->stager);
+  ws_launch(c, ws, blind, ctx->use_graphs, dbg);
+  ZK_CUDA(cudaEventRecord(ws.ev_all, ws.st[0]));
+  ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_all, 0));
+  ws_finish(c, ws, blind, r, s, proof);
+}
+
+void prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* cs, const uint64_t* const* wits,
+                 const size_t* nwits, bool on_device, const uint64_t* rs, const uint64_t* ss,
+                 uint64_t* proofs, int inflight) {
+  ZK_REQUIRE(inflight >= 1 && inflight <= 16, ZK_EINVAL, "batch: in-flight proofs must be 1..16");
+  ZK_REQUIRE(count == 0 || (cs && wits && nwits && proofs), ZK_EINVAL, "batch: NULL argument");
+  const bool blind = rs && ss;
+  for (size_t i = 0; i < count; i++) {
+    ZK_REQUIRE(cs[i] && cs[i]->ctx == ctx, ZK_EINVAL, "batch: circuit from another context");
+    check_job(cs[i], wits[i], nwits[i], blind);
+  }
+  while ((int)ctx->pool.size() < inflight) ctx->pool.emplace_back(new ProveWs());
+  std::vector<long> job(inflight, -1);
+  ZK_CUDA(cudaEventRecord(ctx->ws.ev_begin_pool(), ctx->stream));
+  auto finish = [&](int k) {
+    const long i = job[k];
+    if (i < 0) return;
+    ProveWs& ws = *ctx->pool[k];
+    ws_finish(cs[i], ws, blind, blind ? rs + 4 * i : nullptr, blind ? ss + 4 * i : nullptr,
+              proofs + 32 * i);
+    job[k] = -1;
+  };
+  for (size_t i = 0; i < count; i++) {
+    const int k = (int)(i % inflight);
+    finish(k);  // the slot's previous proof: its host combine overlaps later proofs' GPU work
+    ProveWs& ws = *ctx->pool[k];
+    ws_prepare(cs[i], ws, blind);
+    ZK_CUDA(cudaStreamWaitEvent(ws.st[0], ctx->ws.ev_begin_pool(), 0));
+    ws_stage(cs[i], ws, wits[i], on_device, ctx->stager);
+    ws_launch(cs[i], ws, blind, ctx->use_graphs, nullptr);
+    ZK_CUDA(cudaEventRecord(ws.ev_all, ws.st[0]));
+    ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_all, 0));
+    job[k] = (long)i;
+  }
+  for (int k = 0; k < inflight; k++) finish(k);
 }
 
 }  // namespace zk

@@ -24,6 +24,7 @@
 
 struct zk_circuit {
   zk_ctx* ctx = nullptr;
+  uint64_t id = 0;  // unique per loaded circuit (keys captured graphs)
   uint32_t m1 = 0, l = 0, n = 0;  // nVars, nPublic, domain
   int log_n = 0;
   uint32_t n_coefs = 0;
@@ -71,5 +72,15 @@ int msm_fixed_default_c(size_t n, bool g2);
 // r / s: canonical Fr blinding scalars or nullptr (reference behaviour).
 void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool witness_on_device,
            const uint64_t* r, const uint64_t* s, uint64_t proof[32], ProveIntermediates* dbg);
+
+// Proves `count` jobs (circuits of one context, witnesses host or device)
+// with up to `inflight` proofs on the GPU at once, each on its own workspace
+// and streams; the host combination of one proof overlaps the GPU work of the
+// next ones.  rs / ss: count x 4 u64 blinding scalars or both null.
+void prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* cs, const uint64_t* const* wits,
+                 const size_t* nwits, bool on_device, const uint64_t* rs, const uint64_t* ss,
+                 uint64_t* proofs, int inflight);
+
+uint64_t next_circuit_id();
 
 }  // namespace zk
