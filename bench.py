@@ -61,6 +61,13 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--table-c", default="0,0", help="fixed-base window bits G1,G2 (0 = default)")
     p.add_argument("--workdir", default=os.environ.get("ZK_BENCH_DIR", "/tmp/zyklop_bench"))
+    p.add_argument("--batch-proofs", type=int, default=64, help="0 skips the batched section")
+    p.add_argument("--batch-inflight", type=int, default=4)
+    p.add_argument("--serve-seconds", type=float, default=60.0, help="0 skips serving")
+    p.add_argument("--serve-seconds-fair", type=float, default=20.0)
+    p.add_argument("--serve-rate", type=float, default=200.0)
+    p.add_argument("--serve-logs", default="16,19,21,23")
+    p.add_argument("--serve-inflight", type=int, default=4)
     return p.parse_args()
 
 
@@ -162,20 +169,27 @@ def silenced():
 
 
 # ------------------------------------------------------------- workload
-def circuit_files(args, dist):
-    tag = f"l{args.log_domain}_{args.witness}_s1"
+def synth_cached(args, dist, lg, witness, seed):
+    """Seeded synthetic circuit + witness files, generated once per workdir.
+    uniform: 2 nonzeros per A/B row; circom: 1-4 nonzeros per row and the
+    circom-like witness mix (55% bits, 15% below 2^64, 30% uniform)."""
+    tag = f"l{lg}_{witness}_s{seed}"
     d = os.path.join(args.workdir, tag)
     z, w = os.path.join(d, "circuit.zkey"), os.path.join(d, "witness.wtns")
     done = os.path.join(d, "ok")
     if dist.rank == 0 and not os.path.exists(done):
         os.makedirs(d, exist_ok=True)
         from zyklop_b200 import api
-        nnz = (2, 2) if args.witness == "uniform" else (1, 4)
-        api.synth_circuit(z, w, args.log_domain, n_public=8, n_private_inputs=8, nnz=nnz,
-                          witness=args.witness, seed=1)
+        nnz = (2, 2) if witness == "uniform" else (1, 4)
+        api.synth_circuit(z, w, lg, n_public=8, n_private_inputs=8, nnz=nnz,
+                          witness=witness, seed=seed)
         open(done, "w").write("ok\n")
     dist.barrier()
     return z, w
+
+
+def circuit_files(args, dist):
+    return synth_cached(args, dist, args.log_domain, args.witness, 1)
 
 
 def zkey_bytes(z, sections):
@@ -335,8 +349,173 @@ def run_mine(args, dist):
         "gpu_launches": int(lc1.value - lc0.value),
     }
     circuit.close()
-    check(L.zk_ctx_destroy(ctx))
-    return line, (z, w)
+    return line, (z, w), ctx
+
+
+# --------------------------------------------------------------- batched
+def pct(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def run_batched(args, dist, ctx, L):
+    """64 independent proofs over 8 seeded circuits with log-uniform sizes in
+    [2^14, 2^20] (circom-like witnesses, 1-4 nonzeros per row), all circuits
+    resident with fixed-base tables: zk_prove_batch (several proofs in flight,
+    CUDA-graph replay of each circuit's pipeline) against the same 64 proofs
+    one at a time through zk_prove, and through the one-shot file call."""
+    import torch
+    from zyklop_b200 import api
+    from zyklop_b200._lib import check
+    rng = np.random.default_rng(3)
+    logs = [int(round(x)) for x in rng.uniform(14, 20, 8)]
+    jobs = [int(j) for j in rng.integers(0, 8, args.batch_proofs)]
+    files = [synth_cached(args, dist, lg, "circom", 100 + k) for k, lg in enumerate(logs)]
+    circuits = [api.Circuit(z, ctx=ctx) for z, _ in files]
+    for c in circuits:
+        c.precompute(0, 0)
+    wits = [api.read_wtns(w) for _, w in files]
+    stream = torch.cuda.current_stream()
+    proof = np.zeros(32, np.uint64)
+    pp = proof.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+    def plain_once():
+        lat, out = [], []
+        for j in jobs:
+            t = time.perf_counter()
+            check(L.zk_prove(circuits[j].handle, wits[j].ctypes.data_as(ctypes.c_void_p),
+                             wits[j].shape[0], None, None, pp))
+            lat.append((time.perf_counter() - t) * 1e3)
+            out.append(proof.copy())
+        return lat, out
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    plain_once()  # warm-up: workspaces sized, tables resident
+    (lat, plain_proofs), plain_ms = timed(plain_once)
+    api.set_graphs(True, ctx=ctx)
+    run = lambda: api.prove_batch([circuits[j] for j in jobs], [wits[j] for j in jobs],
+                                  inflight=args.batch_inflight, ctx=ctx)
+    run()  # warm-up: graph capture per (workspace, circuit)
+    batched_proofs, batch_ms = timed(run)
+    api.set_graphs(False, ctx=ctx)
+    assert all(np.array_equal(a, b) for a, b in zip(plain_proofs, batched_proofs)), \
+        "batched proofs differ from one-at-a-time proofs"
+
+    def files_once():
+        for j in jobs:
+            check(L.zk_groth16_prove_files(ctx, files[j][0].encode(), files[j][1].encode(), pp))
+    _, files_ms = timed(files_once)
+    for c in circuits:
+        c.close()
+    n = len(jobs)
+    return {
+        "workload": f"{n} proofs, 8 circuits of 2^{min(logs)}..2^{max(logs)} constraints "
+                    f"(log-uniform, sizes {sorted(logs)}), circom-like witnesses",
+        "batched_proofs_per_s": n / (batch_ms / 1e3),
+        "plain_proofs_per_s": n / (plain_ms / 1e3),
+        "speedup_vs_plain": plain_ms / batch_ms,
+        "plain_files_proofs_per_s": n / (files_ms / 1e3),
+        "speedup_vs_plain_files": files_ms / batch_ms,
+        "plain_latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
+        "batched_call": f"zk_prove_batch, {args.batch_inflight} proofs in flight, CUDA graphs",
+        "plain_call": "zk_prove one at a time (same resident circuits and tables)",
+        "plain_files_call": "zk_groth16_prove_files one at a time (zkey loaded per proof, "
+                            "like the reference's groth16Prove)",
+        "bit_exact": True,
+    }
+
+
+# --------------------------------------------------------------- serving
+def run_serving(args, dist, ctx, L):
+    """Seeded Poisson request stream over 4 resident circuits of 2^16, 2^19,
+    2^21 and 2^23 constraints (mixed 50/25/15/10) through the continuous-
+    batching server (zk_server_*): latency from submit to proof, sustained
+    proofs/s.  The offered rate is first the configured one (above capacity:
+    the queue grows and what is still queued at the end is dropped), then 80%
+    of the sustained rate measured there."""
+    import queue as _queue
+    from zyklop_b200 import api
+    from zyklop_b200 import ZkError
+    logs = [int(x) for x in args.serve_logs.split(",")]
+    mix = [0.5, 0.25, 0.15, 0.10]
+    files = [synth_cached(args, dist, lg, "circom", 200 + k) for k, lg in enumerate(logs)]
+    circuits = [api.Circuit(z, ctx=ctx) for z, _ in files]
+    t = time.perf_counter()
+    for c in circuits:
+        c.precompute(0, 0)
+    t_pre = time.perf_counter() - t
+    wits = [api.read_wtns(w) for _, w in files]
+    alone = [c.prove(w) for c, w in zip(circuits, wits)]  # the reference answer per circuit
+
+    def leg(rate, seconds, seed):
+        rng = np.random.default_rng(seed)
+        srv = api.Server(max_inflight=args.serve_inflight, ctx=ctx)
+        tq = _queue.Queue()
+        lat, done, bad, dropped = [], [0], [0], [0]
+
+        def waiter():
+            while True:
+                item = tq.get()
+                if item is None:
+                    return
+                tk, k = item
+                try:
+                    p, ms = srv.wait(tk)
+                    lat.append(ms)
+                    done[0] += 1
+                    if not np.array_equal(p, alone[k]):
+                        bad[0] += 1
+                except ZkError as e:
+                    if e.code == 10:
+                        dropped[0] += 1
+                    else:
+                        raise
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        t0 = time.perf_counter()
+        at, sent = 0.0, 0
+        while True:
+            at += rng.exponential(1.0 / rate)
+            if at >= seconds:
+                break
+            k = int(rng.choice(4, p=mix))
+            while time.perf_counter() - t0 < at:
+                time.sleep(0.0002)
+            tq.put((srv.submit(circuits[k], wits[k]), k))
+            sent += 1
+        window = time.perf_counter() - t0
+        srv.cancel_queued()
+        tq.put(None)
+        th.join()
+        st = srv.stats()
+        srv.close()
+        return {"offered_req_per_s": rate, "seconds": round(window, 2), "submitted": sent,
+                "completed": done[0], "dropped_unstarted": dropped[0],
+                "sustained_proofs_per_s": done[0] / (time.perf_counter() - t0),
+                "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
+                "peak_inflight": st["peak_inflight"], "admission_waits": st["admission_waits"],
+                "mismatches": bad[0]}
+
+    leg(min(args.serve_rate, 50.0), 2.0, 7)  # warm-up: workspaces grown
+    over = leg(args.serve_rate, args.serve_seconds, 11)
+    fair = leg(0.8 * over["sustained_proofs_per_s"], args.serve_seconds_fair, 13)
+    for c in circuits:
+        c.close()
+    assert over["mismatches"] == 0 and fair["mismatches"] == 0, "served proof differs"
+    return {"workload": f"Poisson requests over circuits 2^{logs[0]}/2^{logs[1]}/2^{logs[2]}/"
+                        f"2^{logs[3]} mixed 50/25/15/10, circom-like witnesses, resident CRS "
+                        f"with fixed-base tables (built in {t_pre:.1f} s)",
+            "server": f"zk_server, up to {args.serve_inflight} proofs in flight, "
+                      "admission by free device memory",
+            "at_offered_rate": over, "at_80pct_of_sustained": fair, "bit_exact": True}
 
 
 # ------------------------------------------------------------- reference
@@ -392,6 +571,11 @@ def run_reference(args, dist):
     }
 
 
+def lib_handle():
+    from zyklop_b200._lib import lib
+    return lib()
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -406,7 +590,12 @@ def main():
         return
     dist = Dist()
     try:
-        line, files = run_mine(args, dist)
+        line, files, ctx = run_mine(args, dist)
+        if dist.world == 1 and args.batch_proofs > 0:
+            line["batched"] = run_batched(args, dist, ctx, lib_handle())
+        if dist.world == 1 and args.serve_seconds > 0:
+            line["serving"] = run_serving(args, dist, ctx, lib_handle())
+        lib_handle().zk_ctx_destroy(ctx)
         if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(*files)
         if dist.rank == 0:

@@ -31,6 +31,7 @@ extern "C" {
 #define ZK_ETIMEOUT 7   /* a bounded wait gave up                      */
 #define ZK_EINTERNAL 8  /* unexpected internal failure                 */
 #define ZK_ENOTSUP 9    /* unsupported parameter                       */
+#define ZK_ECANCELED 10 /* request dropped before it started           */
 
 typedef struct zk_ctx zk_ctx;
 
@@ -235,6 +236,9 @@ int zk_server_wait(zk_server* srv, uint64_t ticket, int timeout_ms, uint64_t* pr
                    double* latency_ms);
 int zk_server_stats(zk_server* srv, uint64_t* completed, uint64_t* failed,
                     uint64_t* peak_inflight, uint64_t* admission_waits);
+/* Drops every request still queued (not yet on the GPU); waiting on one of
+ * them returns ZK_ECANCELED.  Proofs already in flight finish normally. */
+int zk_server_cancel_queued(zk_server* srv, uint64_t* n_cancelled);
 /* Finishes every queued proof, then stops the worker and frees the server. */
 int zk_server_destroy(zk_server* srv);
 

@@ -357,3 +357,43 @@ def test_server_errors(api, files):
             srv.wait(good)  # released
         assert e.value.code == 1
         assert srv.stats()["failed"] == 1
+
+
+def test_server_cancel_queued(api, files):
+    """Requests still queued are dropped with ZK_ECANCELED; the rest finish
+    with the right proof."""
+    from zyklop_b200 import ZkError
+    z, w = files["u16"]
+    c = api.Circuit(z)
+    wit = api.read_wtns(w)
+    ref = c.prove(wit)
+    with api.Server(max_inflight=1) as srv:
+        ts = [srv.submit(c, wit) for _ in range(12)]
+        n = srv.cancel_queued()
+        ok = cancelled = 0
+        for t in ts:
+            try:
+                assert np.array_equal(srv.wait(t)[0], ref)
+                ok += 1
+            except ZkError as e:
+                assert e.code == 10
+                cancelled += 1
+        assert cancelled == n and ok + cancelled == 12
+
+
+def test_twiddle_growth_in_fresh_contexts(api, oracle, files):
+    """Loading a small circuit and then a larger one grows the context's
+    twiddle tables; proofs of both must stay exact in every fresh context."""
+    from zyklop_b200._lib import check, lib
+    L = lib()
+    want = {nm: oracle.prove(blob(files[nm][0]), blob(files[nm][1])) for nm in ("c10", "u16")}
+    for _ in range(4):
+        ctx = ctypes.c_void_p()
+        check(L.zk_ctx_create(0, ctypes.byref(ctx)))
+        try:
+            circ = {nm: api.Circuit(files[nm][0], ctx=ctx) for nm in ("c10", "u16")}
+            for nm, c in circ.items():
+                assert np.array_equal(c.prove(api.read_wtns(files[nm][1])), want[nm]), nm
+                c.close()
+        finally:
+            check(L.zk_ctx_destroy(ctx))

@@ -80,6 +80,7 @@ SIGNATURES = {
     "zk_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, u64p,
                                       ctypes.POINTER(ctypes.c_double)]),
     "zk_server_stats": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_uint64)] * 4),
+    "zk_server_cancel_queued": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "zk_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_groth16_prove_files": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
                                               u64p]),

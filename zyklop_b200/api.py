@@ -348,6 +348,11 @@ class Server:
         return dict(zip(("completed", "failed", "peak_inflight", "admission_waits"),
                         [x.value for x in v]))
 
+    def cancel_queued(self):
+        n = ctypes.c_uint64()
+        check(lib().zk_server_cancel_queued(self.handle, ctypes.byref(n)))
+        return n.value
+
     def close(self):
         if self.handle is not None and self.handle.value:
             check(lib().zk_server_destroy(self.handle))

@@ -271,8 +271,11 @@ void NttTables::ensure(int log_n, cudaStream_t st) {
     hi_t[0] = Fr::one();
     for (size_t i = 1; i < nhi; i++) hi_t[i] = hi_t[i - 1] * step;
     char* base = tmp.as<char>() + dir * (nlo + nhi) * 32;
-    ZK_CUDA(cudaMemcpy(base, hi_t.data(), nhi * 32, cudaMemcpyHostToDevice));
-    ZK_CUDA(cudaMemcpy(base + nhi * 32, lo_t.data(), nlo * 32, cudaMemcpyHostToDevice));
+    // on st, so k_tw_fill is ordered after the copies: a blocking cudaMemcpy
+    // from pageable memory may return before its DMA lands, and st does not
+    // synchronize with the legacy default stream
+    ZK_CUDA(cudaMemcpyAsync(base, hi_t.data(), nhi * 32, cudaMemcpyHostToDevice, st));
+    ZK_CUDA(cudaMemcpyAsync(base + nhi * 32, lo_t.data(), nlo * 32, cudaMemcpyHostToDevice, st));
     fr_t* out = dir ? inv.as<fr_t>() : fwd.as<fr_t>();
     k_tw_fill<<<blocks_for(half), 256, 0, st>>>(out, reinterpret_cast<const fr_t*>(base),
                                                 reinterpret_cast<const fr_t*>(base + nhi * 32),

@@ -147,6 +147,7 @@ void zk_server::run() {
       }
       {
         std::lock_guard<std::mutex> g(mu);
+        if (queue.empty() || queue.front() != r) continue;  // cancelled meanwhile
         queue.pop_front();
       }
       try {
@@ -253,6 +254,22 @@ int zk_server_stats(zk_server* s, uint64_t* completed, uint64_t* failed, uint64_
   if (failed) *failed = s->failed;
   if (peak_inflight) *peak_inflight = s->peak_inflight.load();
   if (admission_waits) *admission_waits = s->admission_waits.load();
+  ZK_API_END
+}
+
+int zk_server_cancel_queued(zk_server* s, uint64_t* n_cancelled) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(s, ZK_EINVAL, "zk_server_cancel_queued: NULL server");
+  std::lock_guard<std::mutex> g(s->mu);
+  const uint64_t n = s->queue.size();
+  for (auto& q : s->queue) {
+    q->status = ZK_ECANCELED;
+    q->error = "request cancelled before it started";
+    q->done = Clock::now();
+  }
+  s->queue.clear();
+  s->cv_done.notify_all();
+  if (n_cancelled) *n_cancelled = n;
   ZK_API_END
 }
 
