@@ -214,6 +214,44 @@ int zk_prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* circuits,
  * proves a circuit and replays it afterwards.  Results are unchanged. */
 int zk_ctx_set_graphs(zk_ctx* ctx, int on);
 
+/* Autotuning.  Each call times candidate settings on seeded synthetic inputs
+ * (points k_i * G, scalars of the given distribution: 0 uniform in Fr, 1 the
+ * circom-like mix of bits and small integers) on the context's stream, checks
+ * that every candidate gives the same result, and records the fastest in the
+ * context for (group, log_n, dist).  Later MSMs and proofs of that size and
+ * distribution use it unless zk_msm_set_config set an explicit window.
+ * Results never change.  No reference counterpart (the reference fixes its
+ * window sizes and bucket tiers at compile time, include/msm_g1.cuh:714-926). */
+typedef struct {
+  int c;         /* window bits (windowed MSMs) */
+  int k0;        /* sorted records per accumulation thread (bucket split threshold) */
+  int k1;        /* partial records per thread in later levels */
+  int chunk;     /* buckets per thread in the bucket reduction */
+  int table_c;   /* fixed-base table window bits (zk_autotune_table_c) */
+  int pass_bits; /* largest NTT pass radix, 2^pass_bits (zk_autotune_ntt) */
+  double ms;     /* time of the chosen setting */
+} zk_tune_result;
+/* Windowed (fixed_c = 0) or fixed-base (fixed_c = table window bits) MSM of
+ * 2^log_n points: window bits, split threshold and reduction chunk. */
+int zk_autotune_msm(zk_ctx* ctx, int group, int log_n, int dist, int fixed_c, zk_tune_result* out);
+/* Fixed-base table window bits for 2^log_n points, tables no larger than
+ * max_table_bytes (0: no cap); used by zk_circuit_precompute(c, 0, 0). */
+int zk_autotune_table_c(zk_ctx* ctx, int group, int log_n, int dist, size_t max_table_bytes,
+                        zk_tune_result* out);
+/* NTT pass radix for the H pipeline at 2^log_n points. */
+int zk_autotune_ntt(zk_ctx* ctx, int log_n, zk_tune_result* out);
+/* The context's tuned settings as text (one entry per line), and back; an
+ * import replaces entries with the same key.  *len receives the text length;
+ * buf may be NULL to query it. */
+int zk_tune_export(zk_ctx* ctx, char* buf, size_t cap, size_t* len);
+int zk_tune_import(zk_ctx* ctx, const char* text);
+/* Scalar distribution hint for zk_msm_g1 / zk_msm_g2 / zk_msm_table_run on
+ * this context (0 uniform, 1 skewed). */
+int zk_ctx_set_scalar_dist(zk_ctx* ctx, int dist);
+/* A circuit's witness distribution: -1 detects it from each host witness
+ * (the default), 0 / 1 fix it. */
+int zk_circuit_set_scalar_dist(zk_circuit* c, int dist);
+
 /* Proof server: continuous batching over resident circuits.  A worker thread
  * keeps up to max_inflight proofs on the GPU, each in its own workspace with
  * its own streams; queued requests are admitted in arrival order as soon as a

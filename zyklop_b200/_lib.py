@@ -73,6 +73,16 @@ SIGNATURES = {
                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                       ctypes.c_void_p, u64p, ctypes.c_int]),
     "zk_ctx_set_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "zk_autotune_msm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_void_p]),
+    "zk_autotune_table_c": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           sz, ctypes.c_void_p]),
+    "zk_autotune_ntt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "zk_tune_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, sz,
+                                      ctypes.POINTER(ctypes.c_size_t)]),
+    "zk_tune_import": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    "zk_ctx_set_scalar_dist": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "zk_circuit_set_scalar_dist": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "zk_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, sz,
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "zk_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, u64p, sz, ctypes.c_void_p,
@@ -99,6 +109,15 @@ class ZkeyHeader(ctypes.Structure):
     _fields_ = [("n_constraints", ctypes.c_uint32), ("n_vars", ctypes.c_uint32),
                 ("n_public", ctypes.c_uint32), ("domain_size", ctypes.c_uint32),
                 ("log_domain", ctypes.c_int32), ("prime", ctypes.c_uint64 * 4)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("c", ctypes.c_int), ("k0", ctypes.c_int), ("k1", ctypes.c_int),
+                ("chunk", ctypes.c_int), ("table_c", ctypes.c_int), ("pass_bits", ctypes.c_int),
+                ("ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class SynthParams(ctypes.Structure):

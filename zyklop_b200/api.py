@@ -147,6 +147,10 @@ class Circuit:
         check(lib().zk_circuit_info(h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         self.n_vars, self.n_public, self.domain = a.value, b.value, c.value
 
+    def set_scalar_dist(self, dist):
+        """-1: detect from each host witness; 0 uniform; 1 skewed"""
+        check(lib().zk_circuit_set_scalar_dist(self.handle, dist))
+
     def precompute(self, c_g1=0, c_g2=0):
         check(lib().zk_circuit_precompute(self.handle, c_g1, c_g2))
 
@@ -297,6 +301,48 @@ def prove_batch(circuits, witnesses, inflight=3, rs=None, ss=None, on_device=Fal
 
 def set_graphs(on, ctx=None):
     check(lib().zk_ctx_set_graphs(ctx, 1 if on else 0))
+
+
+# ------------------------------------------------------------- autotuning
+UNIFORM, SKEWED = 0, 1
+
+
+def autotune_msm(group, log_n, dist=UNIFORM, fixed_c=0, ctx=None):
+    """Time MSM settings at 2^log_n points; the fastest is recorded in ctx."""
+    from ._lib import TuneResult
+    r = TuneResult()
+    check(lib().zk_autotune_msm(ctx, group, log_n, dist, fixed_c, ctypes.byref(r)))
+    return r.as_dict()
+
+
+def autotune_table_c(group, log_n, dist=UNIFORM, max_table_bytes=0, ctx=None):
+    from ._lib import TuneResult
+    r = TuneResult()
+    check(lib().zk_autotune_table_c(ctx, group, log_n, dist, max_table_bytes, ctypes.byref(r)))
+    return r.as_dict()
+
+
+def autotune_ntt(log_n, ctx=None):
+    from ._lib import TuneResult
+    r = TuneResult()
+    check(lib().zk_autotune_ntt(ctx, log_n, ctypes.byref(r)))
+    return r.as_dict()
+
+
+def tune_export(ctx=None):
+    n = ctypes.c_size_t()
+    check(lib().zk_tune_export(ctx, None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    check(lib().zk_tune_export(ctx, buf, n.value + 1, ctypes.byref(n)))
+    return buf.value.decode()
+
+
+def tune_import(text, ctx=None):
+    check(lib().zk_tune_import(ctx, text.encode()))
+
+
+def set_scalar_dist(dist, ctx=None):
+    check(lib().zk_ctx_set_scalar_dist(ctx, dist))
 
 
 def _limbs(x):

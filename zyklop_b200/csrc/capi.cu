@@ -209,8 +209,8 @@ int zk_msm_g1(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uin
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(h_out, ZK_EINVAL, "zk_msm_g1: NULL output");
   ZK_REQUIRE(n == 0 || (d_px && d_py && d_scalars), ZK_EINVAL, "zk_msm_g1: NULL input");
-  const bool inf = msm_g1_run(points_soa(d_px, d_py), d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[0],
-                              ctx->stream, h_out);
+  const bool inf = msm_g1_run(points_soa(d_px, d_py), d_scalars, n, ctx->msm_scratch,
+                              msm_config_for(ctx, false, n, ctx->scalar_dist, 0), ctx->stream, h_out);
   if (is_inf) *is_inf = inf ? 1 : 0;
   ZK_API_END
 }
@@ -222,8 +222,8 @@ int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uin
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(h_out, ZK_EINVAL, "zk_msm_g2: NULL output");
   ZK_REQUIRE(n == 0 || (d_px && d_py && d_scalars), ZK_EINVAL, "zk_msm_g2: NULL input");
-  const bool inf = msm_g2_run(points_soa(d_px, d_py), d_scalars, n, ctx->msm_scratch, ctx->msm_cfg[1],
-                              ctx->stream, h_out);
+  const bool inf = msm_g2_run(points_soa(d_px, d_py), d_scalars, n, ctx->msm_scratch,
+                              msm_config_for(ctx, true, n, ctx->scalar_dist, 0), ctx->stream, h_out);
   if (is_inf) *is_inf = inf ? 1 : 0;
   ZK_API_END
 }
@@ -251,7 +251,7 @@ int zk_msm_scratch_bytes(zk_ctx* ctx, int group, size_t n, size_t* bytes) {
   ctx = resolve_ctx(ctx);
   ZK_REQUIRE(bytes, ZK_EINVAL, "zk_msm_scratch_bytes: NULL output");
   ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_msm_scratch_bytes: group must be 1 or 2");
-  *bytes = msm_scratch_bytes(n, group == 2, ctx->msm_cfg[group - 1]);
+  *bytes = msm_scratch_bytes(n, group == 2, msm_config_for(ctx, group == 2, n, ctx->scalar_dist, 0));
   ZK_API_END
 }
 

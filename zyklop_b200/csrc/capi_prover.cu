@@ -79,7 +79,7 @@ int zk_msm_table_create(zk_ctx* ctx, int group, const uint64_t* d_px, const uint
   t->ctx = ctx;
   t->group = group;
   t->n = n;
-  t->c = c ? c : msm_fixed_default_c(n, group == 2);
+  t->c = c ? c : table_c_for(ctx, group == 2, n, ctx->scalar_dist);
   ZK_REQUIRE(t->c >= 4 && t->c <= 22, ZK_EINVAL, "zk_msm_table_create: c must be 0 or 4..22");
   t->table.ensure(msm_table_bytes(n ? n : 1, group == 2, t->c));
   msm_precompute(group == 2, points_soa(d_px, d_py), n, t->c, t->table.ptr, ctx->stream);
@@ -97,7 +97,7 @@ int zk_msm_table_run(zk_msm_table* t, const uint64_t* d_scalars, size_t n, uint6
   zk_ctx* ctx = enter_ctx(t->ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   const bool g2 = t->group == 2;
-  const MsmConfig& cfg = ctx->msm_cfg[g2 ? 1 : 0];
+  const MsmConfig cfg = msm_config_for(ctx, g2, t->n, ctx->scalar_dist, t->c);
   // the table's records are laid out for t->n points: run over all of them
   // with zero scalars past n (a prefix of the table is not a table)
   const size_t cnt = t->n;

@@ -10,6 +10,7 @@
 #include "ntt.hpp"
 #include "profile.hpp"
 #include "runtime.hpp"
+#include "tune.hpp"
 
 namespace zk {
 
@@ -30,6 +31,7 @@ struct ProveWs {
   DeviceBuffer msm[kStreams];
   PinnedBuffer win[kStreams];
   MsmResult res[kStreams];
+  MsmConfig cfg[kStreams];  // settings of each MSM of the current proof
   // captured pipelines, one per (circuit, blinding); all are dropped when a
   // buffer they point into is reallocated
   struct Graph {
@@ -37,7 +39,8 @@ struct ProveWs {
     uint64_t circuit = 0;  // circuit id the graph was captured for
     bool blind = false;
     int ntt_lmax = 0;  // twiddle table the graph reads
-    MsmConfig cfg[2];  // G1 / G2 MSM settings captured
+    int ntt_bits = 0;  // NTT pass radix captured
+    MsmConfig cfg[kStreams];  // settings of each MSM captured
     int tab_c[2] = {0, 0};  // fixed-base table windows captured (0: windowed)
     uint64_t kernels = 0;
     MsmResult res[kStreams];  // where and how the graph leaves each MSM's windows
@@ -59,7 +62,9 @@ struct zk_ctx {
   zk::NttTables ntt;
   zk::DeviceBuffer ntt_scratch;
   zk::DeviceBuffer msm_scratch;
-  zk::MsmConfig msm_cfg[2];
+  zk::MsmConfig msm_cfg[2];       // explicit settings (c != 0) or defaults
+  zk::TuneTable tune;             // autotuned settings
+  int scalar_dist = 0;            // distribution hint for zk_msm_g1 / g2
   zk::ProveWs ws;
   std::vector<std::unique_ptr<zk::ProveWs>> pool;  // batch workspaces
   bool use_graphs = false;  // replay captured per-circuit proof graphs

@@ -17,7 +17,6 @@ namespace {
 
 constexpr int kTile = 1024;       // elements per pass tile
 constexpr int kPassThreads = 256;
-constexpr int kMaxPassBits = 8;   // radix-2^8 sub-transforms per pass
 
 using host::Fr;
 
@@ -198,9 +197,10 @@ fr_t to_dev(const Fr& x) {
   return r;
 }
 
-// Bit ranges [lo, lo + k) covering [0, L) in near-equal pieces of <= 8 bits.
-int split_passes(int L, int* lo, int* k) {
-  const int np = (L + kMaxPassBits - 1) / kMaxPassBits;
+// Bit ranges [lo, lo + k) covering [0, L) in near-equal pieces of at most
+// maxbits (4..8) bits.
+int split_passes(int L, int maxbits, int* lo, int* k) {
+  const int np = (L + maxbits - 1) / maxbits;
   int at = 0;
   for (int i = 0; i < np; i++) {
     const int bits = (L - at) / (np - i);
@@ -231,16 +231,17 @@ void run_pass(bool dit, const PassArgs& args, int count, const fr_t* tw, int tw_
 
 // all DIF passes (high bit ranges first); first pass may be out of place
 void dif(const PassArgs& first, const PassArgs& rest, int count, const fr_t* tw, int tw_shift, int L,
-         cudaStream_t st) {
+         int maxbits, cudaStream_t st) {
   int lo[8], k[8];
-  const int np = split_passes(L, lo, k);
+  const int np = split_passes(L, maxbits, lo, k);
   for (int i = np - 1; i >= 0; i--)
     run_pass(false, i == np - 1 ? first : rest, count, tw, tw_shift, L, lo[i], k[i], st);
 }
 
-void dit(const PassArgs& args, int count, const fr_t* tw, int tw_shift, int L, cudaStream_t st) {
+void dit(const PassArgs& args, int count, const fr_t* tw, int tw_shift, int L, int maxbits,
+         cudaStream_t st) {
   int lo[8], k[8];
-  const int np = split_passes(L, lo, k);
+  const int np = split_passes(L, maxbits, lo, k);
   for (int i = 0; i < np; i++) run_pass(true, args, count, tw, tw_shift, L, lo[i], k[i], st);
 }
 
@@ -297,7 +298,7 @@ void ntt_inplace(NttTables& tw, uint64_t* a, int log_n, bool inverse, void* scra
   fr_t* s = reinterpret_cast<fr_t*>(scratch);
   PassArgs first{{x, nullptr, nullptr}, {s, nullptr, nullptr}};
   PassArgs rest{{s, nullptr, nullptr}, {s, nullptr, nullptr}};
-  dif(first, rest, 1, table, shift, log_n, st);
+  dif(first, rest, 1, table, shift, log_n, tw.pass_bits[log_n], st);
   const size_t n = size_t(1) << log_n;
   fr_t factor{};
   if (inverse) factor = to_dev(Fr::from_u64(n).inv());
@@ -317,13 +318,13 @@ void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, u
   k_pointwise_mul<<<blocks_for(n), 256, 0, st>>>(A, B, C, n);
   ZK_LAUNCHED();
   PassArgs abc{{A, B, C}, {A, B, C}};
-  dif(abc, abc, 3, tw.inv.as<fr_t>(), shift, log_n, st);
+  dif(abc, abc, 3, tw.inv.as<fr_t>(), shift, log_n, tw.pass_bits[log_n], st);
   const Fr ninv = Fr::from_u64(n).inv();
   const Fr c_odd = ninv * host_root(log_n + 1);
   k_coset_scale<<<dim3(blocks_for(n), 3), 256, 0, st>>>(abc, tw.fwd.as<fr_t>(), shift, log_n,
                                                         to_dev(ninv), to_dev(c_odd));
   ZK_LAUNCHED();
-  dit(abc, 3, tw.fwd.as<fr_t>(), shift, log_n, st);
+  dit(abc, 3, tw.fwd.as<fr_t>(), shift, log_n, tw.pass_bits[log_n], st);
   k_h_final<<<blocks_for(n), 256, 0, st>>>(A, B, C, reinterpret_cast<fr_t*>(h), n);
   ZK_LAUNCHED();
 }

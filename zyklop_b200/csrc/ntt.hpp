@@ -5,7 +5,8 @@
 // w = omega_N = 5^((r-1)/N); the inverse uses w^-1 and scales by 1/N.
 // Elements are Montgomery Fr.
 //
-// Layout of the work: each transform runs as ceil(log N / 8) passes over HBM;
+// Layout of the work: each transform runs as ceil(log N / 8) passes over HBM
+// (8 = the default largest pass radix, tunable per size);
 // a pass loads tiles of up to 256-point sub-transforms (times a few adjacent
 // columns for coalescing) into shared memory, runs up to 8 radix-2 stages there
 // and writes back.  Decimation-in-frequency passes take natural order to
@@ -25,9 +26,16 @@ constexpr int kMaxLogN = 27;  // Fr 2-adicity is 28; H needs omega_2n
 
 // Twiddle tables tw[e] = w^e (forward) and w^-e (inverse), e < 2^(lmax-1),
 // w a primitive 2^lmax-th root.  Smaller transforms read them with a stride.
+// pass_bits[L]: largest radix (2^bits, 4..8) of one shared-memory pass for
+// transforms of 2^L points (a tunable; kernels hold tiles of 1024 points).
+constexpr int kMaxPassBits = 8;
 struct NttTables {
   int lmax = -1;
   DeviceBuffer fwd, inv;
+  int pass_bits[kMaxLogN + 1];
+  NttTables() {
+    for (int& b : pass_bits) b = kMaxPassBits;
+  }
   void ensure(int log_n, cudaStream_t stream);
 };
 

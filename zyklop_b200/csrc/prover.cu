@@ -240,8 +240,8 @@ void circuit_precompute(zk_circuit* c, int c_g1, int c_g2) {
   zk_ctx* ctx = c->ctx;
   cudaStream_t st = ctx->stream;
   const size_t m1 = c->m1, nc = (size_t)c->m1 - c->l - 1, n = c->n;
-  const int g1c = c_g1 ? c_g1 : msm_fixed_default_c(m1 + 1, false);
-  const int g2c = c_g2 ? c_g2 : msm_fixed_default_c(m1 + 1, true);
+  const int g1c = c_g1 ? c_g1 : table_c_for(ctx, false, m1 + 1, c->dist);
+  const int g2c = c_g2 ? c_g2 : table_c_for(ctx, true, m1 + 1, c->dist);
   ZK_REQUIRE(g1c >= 4 && g1c <= 22 && g2c >= 4 && g2c <= 22, ZK_EINVAL,
              "precompute: window bits must be in [4, 22]");
   auto build = [&](DeviceBuffer& tab, const DeviceBuffer& pts, size_t cnt, bool g2, int cb) {
@@ -262,22 +262,33 @@ namespace {
 
 std::atomic<uint64_t> g_circuit_ids{1};
 
-// MSM scratch bytes of each of a proof's MSMs (indexed like ProveWs::msm).
-void ws_scratch_needs(zk_circuit* c, bool blind, size_t need[ProveWs::kStreams]) {
-  zk_ctx* ctx = c->ctx;
-  const size_t m1 = c->m1, n = c->n, l = c->l, nc = m1 - l - 1;
-  const MsmConfig& c1 = ctx->msm_cfg[0];
-  const MsmConfig& c2 = ctx->msm_cfg[1];
+// Settings of each of a proof's MSMs (indexed like ProveWs::msm): H's
+// scalars are NTT outputs (uniform), the others are witness values.
+void ws_msm_configs(zk_circuit* c, MsmConfig cfg[ProveWs::kStreams]) {
+  const zk_ctx* ctx = c->ctx;
+  const size_t m1 = c->m1, nc = m1 - c->l - 1;
+  const int f1 = c->tab_c[0], f2 = c->tab_c[1];
+  cfg[0] = msm_config_for(ctx, false, c->n, kDistUniform, f1);
+  cfg[1] = msm_config_for(ctx, false, m1 + 1, c->dist, f1);
+  cfg[2] = msm_config_for(ctx, true, m1 + 1, c->dist, f2);
+  cfg[3] = msm_config_for(ctx, false, nc, c->dist, f1);
+  cfg[4] = msm_config_for(ctx, false, m1 + 1, c->dist, f1);
+}
+
+// MSM scratch bytes of each of a proof's MSMs.
+void ws_scratch_needs(zk_circuit* c, bool blind, const MsmConfig cfg[ProveWs::kStreams],
+                      size_t need[ProveWs::kStreams]) {
+  const size_t m1 = c->m1, n = c->n, nc = m1 - c->l - 1;
   const bool fixed = c->tab_c[0] != 0;
-  auto scratch = [&](size_t cnt, bool g2) {
-    return fixed ? msm_scratch_bytes_fixed(cnt, g2, c->tab_c[g2 ? 1 : 0], g2 ? c2 : c1)
-                 : msm_scratch_bytes(cnt, g2, g2 ? c2 : c1);
+  auto scratch = [&](int i, size_t cnt, bool g2) {
+    return fixed ? msm_scratch_bytes_fixed(cnt, g2, c->tab_c[g2 ? 1 : 0], cfg[i])
+                 : msm_scratch_bytes(cnt, g2, cfg[i]);
   };
-  need[0] = scratch(n, false);
-  need[1] = scratch(m1 + 1, false);
-  need[2] = scratch(m1 + 1, true);
-  need[3] = scratch(nc, false);
-  need[4] = blind ? scratch(m1 + 1, false) : 0;
+  need[0] = scratch(0, n, false);
+  need[1] = scratch(1, m1 + 1, false);
+  need[2] = scratch(2, m1 + 1, true);
+  need[3] = scratch(3, nc, false);
+  need[4] = blind ? scratch(4, m1 + 1, false) : 0;
 }
 
 // Sizes the workspace for this circuit (buffers, MSM scratch, result copies).
@@ -285,8 +296,9 @@ void ws_prepare(zk_circuit* c, ProveWs& ws, bool blind) {
   zk_ctx* ctx = c->ctx;
   ws.init();
   const size_t m1 = c->m1, n = c->n;
+  ws_msm_configs(c, ws.cfg);
   size_t need[ProveWs::kStreams];
-  ws_scratch_needs(c, blind, need);
+  ws_scratch_needs(c, blind, ws.cfg, need);
   const bool grow = ws.we.cap < 32 * (m1 + 1) || ws.aw.cap < 32 * n ||
                     [&] {
                       for (int i = 0; i < ProveWs::kStreams; i++)
@@ -329,8 +341,6 @@ void ws_stage(zk_circuit* c, ProveWs& ws, const uint64_t* witness, bool on_devic
 void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg) {
   zk_ctx* ctx = c->ctx;
   const size_t m1 = c->m1, n = c->n, l = c->l, nc = m1 - l - 1;
-  const MsmConfig& c1 = ctx->msm_cfg[0];
-  const MsmConfig& c2 = ctx->msm_cfg[1];
   const bool fixed = c->tab_c[0] != 0;
   cudaStream_t s0 = ws.st[0];
   uint64_t* we = ws.we.as<uint64_t>();
@@ -342,13 +352,13 @@ void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg
     if (si) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
     if (fixed)
       ws.res[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
-                                    ws.msm[i].cap, g2 ? c2 : c1, st);
+                                    ws.msm[i].cap, ws.cfg[i], st);
     else if (g2)
       ws.res[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr,
-                                 ws.msm[i].cap, c2, st);
+                                 ws.msm[i].cap, ws.cfg[i], st);
     else
       ws.res[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr,
-                                 ws.msm[i].cap, c1, st);
+                                 ws.msm[i].cap, ws.cfg[i], st);
     ZK_REQUIRE(ws.res[i].bytes <= kMaxWindowBytes, ZK_EINTERNAL, "prove: MSM result too large");
     ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, ws.res[i].d_data, ws.res[i].bytes,
                             cudaMemcpyDeviceToHost, st));
@@ -391,12 +401,16 @@ void ws_launch(zk_circuit* c, ProveWs& ws, bool blind, bool use_graph, ProveInte
     return;
   }
   const zk_ctx* ctx = c->ctx;
-  const int lmax = ctx->ntt.lmax;
+  const int lmax = ctx->ntt.lmax, bits = ctx->ntt.pass_bits[c->log_n];
+  auto same_cfg = [&](const ProveWs::Graph& x) {
+    for (int i = 0; i < ProveWs::kStreams; i++)
+      if (!(x.cfg[i] == ws.cfg[i])) return false;
+    return true;
+  };
   ProveWs::Graph* gr = nullptr;
   for (ProveWs::Graph& x : ws.graphs)
-    if (x.circuit == c->id && x.blind == blind && x.ntt_lmax == lmax &&
-        x.cfg[0] == ctx->msm_cfg[0] && x.cfg[1] == ctx->msm_cfg[1] && x.tab_c[0] == c->tab_c[0] &&
-        x.tab_c[1] == c->tab_c[1])
+    if (x.circuit == c->id && x.blind == blind && x.ntt_lmax == lmax && x.ntt_bits == bits &&
+        same_cfg(x) && x.tab_c[0] == c->tab_c[0] && x.tab_c[1] == c->tab_c[1])
       gr = &x;
   if (!gr) {
     if (ws.graphs.size() >= ProveWs::kMaxGraphs) {
@@ -426,8 +440,8 @@ void ws_launch(zk_circuit* c, ProveWs& ws, bool blind, bool use_graph, ProveInte
     x.circuit = c->id;
     x.blind = blind;
     x.ntt_lmax = lmax;
-    x.cfg[0] = ctx->msm_cfg[0];
-    x.cfg[1] = ctx->msm_cfg[1];
+    x.ntt_bits = bits;
+    for (int i = 0; i < ProveWs::kStreams; i++) x.cfg[i] = ws.cfg[i];
     x.tab_c[0] = c->tab_c[0];
     x.tab_c[1] = c->tab_c[1];
     for (int i = 0; i < ProveWs::kStreams; i++) x.res[i] = ws.res[i];
@@ -473,13 +487,21 @@ void check_job(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool bl
   ZK_REQUIRE(!blind || c->has_b1, ZK_EFORMAT, "blinding needs zkey section 6 (B1 points)");
 }
 
+// A host witness tells the circuit's scalar distribution (it keys the tuned
+// MSM settings); device witnesses keep the last one seen.
+void note_witness(zk_circuit* c, const uint64_t* witness, bool on_device) {
+  if (c->dist_auto && !on_device) c->dist = detect_scalar_dist(witness, c->m1);
+}
+
 }  // namespace
 
 // Device bytes that preparing ws for this circuit would newly allocate (the
 // proof server admits a request only when that much memory is free).
 size_t ws_bytes_needed(zk_circuit* c, const ProveWs& ws, bool blind) {
+  MsmConfig cfg[ProveWs::kStreams];
+  ws_msm_configs(c, cfg);
   size_t need[ProveWs::kStreams];
-  ws_scratch_needs(c, blind, need);
+  ws_scratch_needs(c, blind, cfg, need);
   const size_t m1 = c->m1, n = c->n;
   auto grow = [](const DeviceBuffer& b, size_t want) { return b.cap < want ? want : size_t(0); };
   size_t total = grow(ws.we, 32 * (m1 + 1)) + grow(ws.aw, 32 * n) + grow(ws.bw, 32 * n) +
@@ -491,6 +513,7 @@ size_t ws_bytes_needed(zk_circuit* c, const ProveWs& ws, bool blind) {
 
 // Starts a proof from a host witness on ws's streams without waiting for it.
 void ws_submit(zk_circuit* c, ProveWs& ws, const uint64_t* witness, bool blind, Stager& stager) {
+  note_witness(c, witness, false);
   ws_prepare(c, ws, blind);
   ws_stage(c, ws, witness, false, stager);
   ws_launch(c, ws, blind, c->ctx->use_graphs, nullptr);
@@ -519,6 +542,7 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   check_job(c, witness, n_witness, blind);
   zk_ctx* ctx = c->ctx;
   ProveWs& ws = ctx->ws;
+  note_witness(c, witness, on_device);
   ws_prepare(c, ws, blind);
   // the proof starts after prior work on the context stream and ends before
   // later work on it, so callers can bracket it with events on that stream
@@ -556,6 +580,7 @@ void prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* cs, const uint64_
     const int k = (int)(i % inflight);
     finish(k);  // the slot's previous proof: its host combine overlaps later proofs' GPU work
     ProveWs& ws = *ctx->pool[k];
+    note_witness(cs[i], wits[i], on_device);
     ws_prepare(cs[i], ws, blind);
     ZK_CUDA(cudaStreamWaitEvent(ws.st[0], ctx->ws.ev_begin_pool(), 0));
     ws_stage(cs[i], ws, wits[i], on_device, ctx->stager);

@@ -31,6 +31,10 @@ struct zk_circuit {
   uint64_t alpha1[8], beta1[8], beta2[16], gamma2[16], delta1[8], delta2[16];
   std::vector<uint64_t> ic;  // (l + 1) x 8, empty if the zkey has no section 3
   bool has_b1 = false;
+  // witness scalar distribution (keys autotuned MSM settings); detected from
+  // host witnesses unless set explicitly
+  int dist = 0;
+  bool dist_auto = true;
   // CRS points, AoS (x, y) records; A / B1 / B2 carry alpha1 / beta1 / beta2
   // as record 0, like the reference's extended buffers (src/groth16.cu:1199-1227)
   zk::DeviceBuffer pts_a, pts_b1, pts_b2, pts_c, pts_h;
