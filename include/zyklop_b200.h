@@ -56,6 +56,11 @@ int zk_ctx_sync(zk_ctx* ctx);
  * and finishes before work queued after it, so events recorded there bracket
  * whole proofs.  Only for contexts from zk_ctx_create. */
 int zk_ctx_set_stream(zk_ctx* ctx, void* stream);
+/* Device buffers come from a per-device stream-ordered pool that keeps freed
+ * blocks for reuse (loading and freeing circuits then costs no driver
+ * mapping work).  This returns the pool's unused blocks on the context's
+ * device to the driver. */
+int zk_release_cached_memory(zk_ctx* ctx);
 
 /* ---- measurement ----------------------------------------------------------- */
 /* Number of kernels this library has launched in the process so far. */
@@ -254,10 +259,10 @@ int zk_circuit_set_scalar_dist(zk_circuit* c, int dist);
 
 /* Proof server: continuous batching over resident circuits.  A worker thread
  * keeps up to max_inflight proofs on the GPU, each in its own workspace with
- * its own streams; queued requests are admitted in arrival order as soon as a
- * workspace is free and the device has room for its buffers plus
- * reserve_bytes (admission by free memory), so a request that arrives while
- * others run overlaps with them.  Each proof equals the one zk_prove gives
+ * its own streams; queued requests are admitted (in the order
+ * zk_server_set_policy picks) as soon as a workspace is free and the device
+ * has room for its buffers plus reserve_bytes (admission by free memory), so
+ * a request that arrives while others run overlaps with them.  Each proof equals the one zk_prove gives
  * for the same job.  The witness buffer and the circuit must stay valid until
  * zk_server_wait returns for that ticket.  No reference counterpart (the
  * reference proves one file pair per process). */
@@ -274,6 +279,10 @@ int zk_server_wait(zk_server* srv, uint64_t ticket, int timeout_ms, uint64_t* pr
                    double* latency_ms);
 int zk_server_stats(zk_server* srv, uint64_t* completed, uint64_t* failed,
                     uint64_t* peak_inflight, uint64_t* admission_waits);
+/* Admission order: policy 0 = arrival order; policy 1 (the default) = the
+ * smallest circuit among the first 64 queued requests, except that a request
+ * queued for longer than max_wait_ms (default 500) goes first. */
+int zk_server_set_policy(zk_server* srv, int policy, int max_wait_ms);
 /* Drops every request still queued (not yet on the GPU); waiting on one of
  * them returns ZK_ECANCELED.  Proofs already in flight finish normally. */
 int zk_server_cancel_queued(zk_server* srv, uint64_t* n_cancelled);

@@ -397,3 +397,29 @@ def test_twiddle_growth_in_fresh_contexts(api, oracle, files):
                 c.close()
         finally:
             check(L.zk_ctx_destroy(ctx))
+
+
+def test_server_admits_small_circuits_first(api, files):
+    """Policy 1 admits the smallest queued circuit next (aging aside), so a
+    small proof queued behind large ones finishes before them; policy 0
+    keeps arrival order.  Results are unchanged either way."""
+    import time
+    big, small = api.Circuit(files["u16"][0]), api.Circuit(files["u10"][0])
+    wb, ws = api.read_wtns(files["u16"][1]), api.read_wtns(files["u10"][1])
+    ref_b, ref_s = big.prove(wb), small.prove(ws)
+    for policy in (1, 0):
+        with api.Server(max_inflight=1) as srv:
+            srv.set_policy(policy, max_wait_ms=60000)
+            jobs = [(big, wb, ref_b)] * 4 + [(small, ws, ref_s)]
+            sub = []
+            for c, w, ref in jobs:
+                sub.append((time.perf_counter(), srv.submit(c, w), ref))
+            done = []
+            for t0, tk, ref in sub:
+                p, lat = srv.wait(tk)
+                assert np.array_equal(p, ref)
+                done.append(t0 + lat / 1e3)
+        if policy == 1:
+            assert done[4] < done[3]
+        else:
+            assert done[4] > done[3]

@@ -27,6 +27,7 @@ SIGNATURES = {
     "zk_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_ctx_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_ctx_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "zk_release_cached_memory": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64)]),
     "zk_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "zk_ctx_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
@@ -90,6 +91,7 @@ SIGNATURES = {
     "zk_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, u64p,
                                       ctypes.POINTER(ctypes.c_double)]),
     "zk_server_stats": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_uint64)] * 4),
+    "zk_server_set_policy": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "zk_server_cancel_queued": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "zk_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_groth16_prove_files": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,

@@ -394,6 +394,10 @@ class Server:
         return dict(zip(("completed", "failed", "peak_inflight", "admission_waits"),
                         [x.value for x in v]))
 
+    def set_policy(self, policy, max_wait_ms=500):
+        """0: arrival order; 1: smallest circuit first with aging"""
+        check(lib().zk_server_set_policy(self.handle, policy, max_wait_ms))
+
     def cancel_queued(self):
         n = ctypes.c_uint64()
         check(lib().zk_server_cancel_queued(self.handle, ctypes.byref(n)))

@@ -111,6 +111,14 @@ int zk_ctx_set_stream(zk_ctx* ctx, void* stream) {
   ZK_API_END
 }
 
+int zk_release_cached_memory(zk_ctx* ctx) {
+  ZK_API_BEGIN
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  release_cached_memory();
+  ZK_API_END
+}
+
 int zk_launch_count(uint64_t* out) {
   ZK_API_BEGIN
   ZK_REQUIRE(out, ZK_EINVAL, "zk_launch_count: NULL output");

@@ -27,11 +27,88 @@ const char* last_error() { return g_last_error.c_str(); }
   throw Error(e == cudaErrorMemoryAllocation ? ZK_ENOMEM : ZK_ECUDA, buf);
 }
 
+namespace {
+// One stream-ordered pool per device for every DeviceBuffer: freed blocks stay
+// reserved (release threshold = all) and later allocations reuse them without
+// the driver mapping or unmapping pages, which is most of what loading and
+// freeing a circuit through cudaMalloc / cudaFree would cost.
+constexpr int kMaxPoolDevices = 64;
+struct DevPool {
+  std::once_flag once;
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t st = nullptr;  // allocation / free stream (synchronized on use)
+  bool ok = false;
+};
+DevPool g_pools[kMaxPoolDevices];
+
+DevPool* pool_of(int dev) {
+  if (dev < 0 || dev >= kMaxPoolDevices) return nullptr;
+  DevPool& p = g_pools[dev];
+  std::call_once(p.once, [&] {
+    int supported = 0;
+    if (cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev) != cudaSuccess ||
+        !supported) {
+      (void)cudaGetLastError();
+      return;
+    }
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (cudaMemPoolCreate(&p.pool, &props) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return;
+    }
+    uint64_t keep = ~uint64_t(0);
+    cudaMemPoolSetAttribute(p.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (cudaStreamCreateWithFlags(&p.st, cudaStreamNonBlocking) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return;
+    }
+    p.ok = true;
+  });
+  return p.ok ? &p : nullptr;
+}
+}  // namespace
+
+size_t device_free_bytes() {
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (DevPool* p = pool_of(dev)) {
+    uint64_t reserved = 0, used = 0;
+    cudaMemPoolGetAttribute(p->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(p->pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    if (reserved > used) fr += reserved - used;
+  }
+  return fr;
+}
+
+void release_cached_memory() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (DevPool* p = pool_of(dev)) {
+    cudaStreamSynchronize(p->st);
+    cudaMemPoolTrimTo(p->pool, 0);
+  }
+}
+
 void DeviceBuffer::ensure(size_t bytes) {
   if (bytes <= cap && ptr) return;
   release();
   size_t want = align256(bytes ? bytes : 256);
-  cudaError_t e = cudaMalloc(&ptr, want);
+  cudaGetDevice(&dev);
+  cudaError_t e;
+  if (DevPool* p = pool_of(dev)) {
+    e = cudaMallocFromPoolAsync(&ptr, want, p->pool, p->st);
+    // the block is usable from any stream once the allocation has executed
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->st);
+    pooled = true;
+  } else {
+    e = cudaMalloc(&ptr, want);
+    pooled = false;
+  }
   if (e != cudaSuccess) {
     ptr = nullptr;
     cap = 0;
@@ -44,7 +121,19 @@ void DeviceBuffer::ensure(size_t bytes) {
 }
 
 void DeviceBuffer::release() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    if (pooled) {
+      int cur = 0;
+      cudaGetDevice(&cur);
+      if (cur != dev) cudaSetDevice(dev);
+      // like cudaFree: no work still using the block may run after it is reused
+      cudaDeviceSynchronize();
+      if (DevPool* p = pool_of(dev)) cudaFreeAsync(ptr, p->st);
+      if (cur != dev) cudaSetDevice(cur);
+    } else {
+      cudaFree(ptr);
+    }
+  }
   ptr = nullptr;
   cap = 0;
 }

@@ -50,12 +50,20 @@ void count_launch(int n);
 
 void set_last_error(int code, const char* msg);
 
+// Free device memory on the current device, counting blocks the library's
+// pool holds for reuse.
+size_t device_free_bytes();
+// Returns the pool's unused blocks on the current device to the driver.
+void release_cached_memory();
+
 // Growable device allocation.  ensure() keeps the old allocation when it is
 // large enough; growing frees the old one first (callers synchronize the
 // streams that used it before growing).
 struct DeviceBuffer {
   void* ptr = nullptr;
   size_t cap = 0;
+  int dev = 0;          // device the block lives on
+  bool pooled = false;  // from the device's stream-ordered pool
   DeviceBuffer() = default;
   DeviceBuffer(const DeviceBuffer&) = delete;
   DeviceBuffer& operator=(const DeviceBuffer&) = delete;

@@ -10,6 +10,7 @@
 // reference proves one file pair per process.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -71,10 +72,24 @@ struct zk_server {
   zk::Stager stager;
   std::thread worker;
   // statistics
+  // admission order: 0 arrival order; 1 smallest circuit first among the
+  // first kLookahead queued, except that a request older than max_wait goes
+  // first (no starvation)
+  static constexpr size_t kLookahead = 64;
+  int policy = 1;
+  std::chrono::milliseconds max_wait{500};
   uint64_t completed = 0, failed = 0;  // under mu
   std::atomic<uint64_t> peak_inflight{0}, admission_waits{0};  // written by the worker
 
   void run();
+  size_t pick_locked() const {
+    if (policy == 0 || Clock::now() - queue.front()->submitted > max_wait) return 0;
+    size_t best = 0;
+    const size_t look = std::min(queue.size(), kLookahead);
+    for (size_t i = 1; i < look; i++)
+      if (queue[i]->circuit->n < queue[best]->circuit->n) best = i;
+    return best;
+  }
   void deliver(const std::shared_ptr<Request>& r, int status, const std::string& err) {
     std::lock_guard<std::mutex> g(mu);
     r->status = status;
@@ -115,7 +130,7 @@ void zk_server::run() {
       {
         std::unique_lock<std::mutex> g(mu);
         if (queue.empty()) break;
-        r = queue.front();
+        r = queue[pick_locked()];
       }
       Slot* free_slot = nullptr;
       for (Slot& sl : slots)
@@ -135,8 +150,7 @@ void zk_server::run() {
         need = 0;
       }
       if (need) {
-        size_t fr = 0, tot = 0;
-        cudaMemGetInfo(&fr, &tot);
+        const size_t fr = zk::device_free_bytes();
         if (fr < need + reserve) {
           if (busy > 0) {  // wait for running proofs to release memory
             if (!r->waited) admission_waits++;
@@ -147,8 +161,9 @@ void zk_server::run() {
       }
       {
         std::lock_guard<std::mutex> g(mu);
-        if (queue.empty() || queue.front() != r) continue;  // cancelled meanwhile
-        queue.pop_front();
+        const auto it = std::find(queue.begin(), queue.end(), r);
+        if (it == queue.end()) continue;  // cancelled meanwhile
+        queue.erase(it);
       }
       try {
         if (r->n_witness < r->circuit->m1)
@@ -254,6 +269,17 @@ int zk_server_stats(zk_server* s, uint64_t* completed, uint64_t* failed, uint64_
   if (failed) *failed = s->failed;
   if (peak_inflight) *peak_inflight = s->peak_inflight.load();
   if (admission_waits) *admission_waits = s->admission_waits.load();
+  ZK_API_END
+}
+
+int zk_server_set_policy(zk_server* s, int policy, int max_wait_ms) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(s, ZK_EINVAL, "zk_server_set_policy: NULL server");
+  ZK_REQUIRE(policy == 0 || policy == 1, ZK_EINVAL, "zk_server_set_policy: policy 0 or 1");
+  ZK_REQUIRE(max_wait_ms >= 0, ZK_EINVAL, "zk_server_set_policy: negative wait");
+  std::lock_guard<std::mutex> g(s->mu);
+  s->policy = policy;
+  s->max_wait = std::chrono::milliseconds(max_wait_ms);
   ZK_API_END
 }
 
