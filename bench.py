@@ -62,7 +62,9 @@ def parse_args():
     p.add_argument("--table-c", default="0,0", help="fixed-base window bits G1,G2 (0 = default)")
     p.add_argument("--workdir", default=os.environ.get("ZK_BENCH_DIR", "/tmp/zyklop_bench"))
     p.add_argument("--batch-proofs", type=int, default=64, help="0 skips the batched section")
-    p.add_argument("--batch-inflight", type=int, default=4)
+    p.add_argument("--batch-inflight", type=int, default=8)
+    p.add_argument("--no-autotune", action="store_true",
+                   help="skip the autotuner (default settings for every size)")
     p.add_argument("--serve-seconds", type=float, default=60.0, help="0 skips serving")
     p.add_argument("--serve-seconds-fair", type=float, default=20.0)
     p.add_argument("--serve-rate", type=float, default=200.0)
@@ -231,6 +233,36 @@ def cpu_baseline(z, w):
 
 
 # ------------------------------------------------------------------ mine
+def traffic_per_point():
+    """DRAM bytes per point of one accumulation launch (ncu summary)."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "traffic_per_point.txt")
+    if os.path.exists(path):
+        for line in open(path):
+            f = line.split()
+            if len(f) == 2 and not line.startswith("#"):
+                out[f[0]] = float(f[1])
+    return out
+
+
+def roofline_of(kind, rec, peak, step_ms):
+    """Algorithmic IMAD-class ops of the accumulation kernels of `kind` over
+    their measured event time, against the measured IMAD peak."""
+    kms, kl, ku = rec
+    if not kl or kms <= 0:
+        return None
+    achieved = ku * FP_MULTS_PER_POINT[kind] * IMAD_PER_FP_MULT / (kms / 1e3) / 1e12
+    per_point = traffic_per_point().get(kind)
+    r = {"bound": "imad", "kernel": f"k_msm_accum0 ({kind})", "achieved": achieved,
+         "peak": peak, "unit": "TIOP/s", "frac": achieved / peak,
+         "traffic": per_point * ku / kl if per_point else None,
+         "peak_source": "zk_imad_probe (measured carry-chain IMAD throughput)",
+         "avg_launch_ms": kms / kl, "launches": int(kl)}
+    if step_ms:
+        r["share_of_step"] = kms / step_ms
+    return r
+
+
 def run_mine(args, dist):
     import torch
     torch.cuda.set_device(dist.local)
@@ -242,7 +274,12 @@ def run_mine(args, dist):
     check(L.zk_ctx_create(dist.local, ctypes.byref(ctx)))
     stream = torch.cuda.current_stream()
     check(L.zk_ctx_set_stream(ctx, ctypes.c_void_p(stream.cuda_stream)))
+    t_tune = time.perf_counter()
+    tuned = autotune_sizes(args, api, ctx, [args.log_domain],
+                           api.UNIFORM if args.witness == "uniform" else api.SKEWED)
+    t_tune = time.perf_counter() - t_tune
     circuit = api.Circuit(z, ctx=ctx)
+    circuit.prove(api.read_wtns(w))  # detects the witness distribution
     t_pre = time.perf_counter()
     tc = [int(x) for x in args.table_c.split(",")]
     circuit.precompute(tc[0], tc[1])  # fixed-base window tables for the resident CRS
@@ -286,30 +323,36 @@ def run_mine(args, dist):
     assert np.array_equal(proof, reference_proof), "proofs changed between steps"
     value = args.gpus * args.steps / (ms / 1e3)
 
-    # roofline of the dominant kernel kind
+    # roofline of the dominant kernel kind, from the timed region (the five
+    # MSM streams of a proof overlap, so each launch's event time includes
+    # time shared with the other streams)
     kinds = {k: (prof.ms[i], prof.launches[i], prof.units[i]) for i, k in enumerate(Profile.KINDS)}
     dom = max(FP_MULTS_PER_POINT, key=lambda k: kinds[k][0])
-    kms, kl, ku = kinds[dom]
-    achieved = ku * FP_MULTS_PER_POINT[dom] * IMAD_PER_FP_MULT / (kms / 1e3) / 1e12
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic_per_point.json")
-    if os.path.exists(tfile):
-        per_point = json.load(open(tfile)).get(dom)
-        if per_point:
-            traffic = per_point * ku / kl
-    roofline = {"bound": "imad", "kernel": f"k_msm_accum0 ({dom})", "achieved": achieved,
-                "peak": peak.value, "unit": "TIOP/s", "frac": achieved / peak.value,
-                "traffic": traffic,
-                "peak_source": "zk_imad_probe (measured carry-chain IMAD throughput)",
-                "avg_launch_ms": kms / kl, "launches": int(kl),
-                "share_of_step": kms / ms}
+    roofline = roofline_of(dom, kinds[dom], peak.value, ms)
     other = {k: {"ms_per_step": v[0] / args.steps, "launches": int(v[1])} for k, v in kinds.items()}
+
+    # the same kernels with a proof's MSMs back to back on one stream (an
+    # extra, untimed pass): event times are then the kernels' own durations
+    check(L.zk_ctx_set_prove_streams(ctx, 1))
+    step()
+    torch.cuda.synchronize()
+    check(L.zk_ctx_set_profiling(ctx, 1))
+    check(L.zk_ctx_profile(ctx, ctypes.byref(prof)))  # clear
+    for _ in range(min(args.steps, 3)):
+        step()
+    torch.cuda.synchronize()
+    check(L.zk_ctx_profile(ctx, ctypes.byref(prof)))
+    check(L.zk_ctx_set_profiling(ctx, 0))
+    check(L.zk_ctx_set_prove_streams(ctx, 0))
+    assert np.array_equal(proof, reference_proof), "proofs changed with one MSM stream"
+    skinds = {k: (prof.ms[i], prof.launches[i], prof.units[i]) for i, k in enumerate(Profile.KINDS)}
+    roofline_serial = {k: roofline_of(k, skinds[k], peak.value, None) for k in FP_MULTS_PER_POINT}
 
     # e2e through the one-shot host-buffer entry point
     e2e_steps = args.e2e_steps or min(args.steps, 5)
     h2d = zkey_bytes(z, {4, 5, 6, 7, 8, 9}) + os.path.getsize(w)
-    W1, W2 = 17, 17
-    d2h = 256 + 4 * 128 * W1 + 256 * W2
+    W1, W2 = 17, 17  # windows of the windowed MSMs at 2^20 (16-bit windows)
+    d2h = 3 * 2 * 128 * W1 + 2 * 256 * W2  # (U, A) pairs per window: A, C, H and B2
     check(L.zk_groth16_prove_files(ctx, z.encode(), w.encode(), pp))  # warm the page cache
     assert np.array_equal(proof, reference_proof)
     dist.barrier()
@@ -336,20 +379,45 @@ def run_mine(args, dist):
         "data": "synthetic (seeded circuit, CRS and witness)",
         "config": dict(config(args, circuit.n_vars, circuit.domain),
                        resident_crs="zkey uploaded once; fixed-base window tables built once "
-                                    f"({t_pre:.2f} s, zk_circuit_precompute)"),
+                                    f"({t_pre:.2f} s, zk_circuit_precompute)",
+                       autotuned=tuned, autotune_s=round(t_tune, 1)),
         "e2e": {"value": args.gpus * e2e_steps / (ems / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "call": "zk_groth16_prove_files (zkey + wtns files -> proof)"},
         "e2e_resident": {"value": args.gpus * e2e_steps / (rms / 1e3), "unit": UNIT,
-                         "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": d2h,
+                         "h2d_bytes_per_step": 32 * n,
+                         "d2h_bytes_per_step": 3 * 2 * 128 + 2 * 256,  # one (U, A) per MSM
                          "call": "zk_prove (resident circuit, host witness)"},
         "roofline": roofline,
+        "roofline_serial_msm": roofline_serial,
         "kernels": other,
         "clocks": clk,
         "gpu_launches": int(lc1.value - lc0.value),
     }
     circuit.close()
     return line, (z, w), ctx
+
+
+# -------------------------------------------------------------- autotuning
+def autotune_sizes(args, api, ctx, logs, witness_dist, max_table_bytes=16 << 30, table_upto=21):
+    """Fixed-base table window bits and MSM settings for circuits of 2^lg
+    constraints: witness MSMs with the witness distribution, H with uniform
+    scalars.  Table sizes are searched up to 2^table_upto points (larger
+    ones keep the default window bits).  Returns the tuned entries."""
+    if args.no_autotune:
+        return "defaults"
+    from zyklop_b200.api import table_c_default
+    for lg in logs:
+        for g in (1, 2):
+            if lg <= table_upto:
+                tc = api.autotune_table_c(g, lg, witness_dist, max_table_bytes=max_table_bytes,
+                                          ctx=ctx)["table_c"]
+            else:
+                tc = table_c_default(lg)
+            api.autotune_msm(g, lg, witness_dist, fixed_c=tc, ctx=ctx)
+            if g == 1 and witness_dist != api.UNIFORM:
+                api.autotune_msm(g, lg, api.UNIFORM, fixed_c=tc, ctx=ctx)
+    return api.tune_export(ctx=ctx).strip().splitlines()
 
 
 # --------------------------------------------------------------- batched
@@ -370,10 +438,14 @@ def run_batched(args, dist, ctx, L):
     logs = [int(round(x)) for x in rng.uniform(14, 20, 8)]
     jobs = [int(j) for j in rng.integers(0, 8, args.batch_proofs)]
     files = [synth_cached(args, dist, lg, "circom", 100 + k) for k, lg in enumerate(logs)]
+    t_tune = time.perf_counter()
+    tuned = autotune_sizes(args, api, ctx, sorted(set(logs)), api.SKEWED)
+    t_tune = time.perf_counter() - t_tune
     circuits = [api.Circuit(z, ctx=ctx) for z, _ in files]
-    for c in circuits:
-        c.precompute(0, 0)
     wits = [api.read_wtns(w) for _, w in files]
+    for c, w in zip(circuits, wits):
+        c.prove(w)  # detects the witness distribution (keys the tuned settings)
+        c.precompute(0, 0)
     stream = torch.cuda.current_stream()
     proof = np.zeros(32, np.uint64)
     pp = proof.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
@@ -425,6 +497,7 @@ def run_batched(args, dist, ctx, L):
         "speedup_vs_plain_files": files_ms / batch_ms,
         "plain_latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
         "batched_call": f"zk_prove_batch, {args.batch_inflight} proofs in flight, CUDA graphs",
+        "autotuned": tuned, "autotune_s": round(t_tune, 1),
         "plain_call": "zk_prove one at a time (same resident circuits and tables)",
         "plain_files_call": "zk_groth16_prove_files one at a time (zkey loaded per proof, "
                             "like the reference's groth16Prove)",
@@ -446,12 +519,16 @@ def run_serving(args, dist, ctx, L):
     logs = [int(x) for x in args.serve_logs.split(",")]
     mix = [0.5, 0.25, 0.15, 0.10]
     files = [synth_cached(args, dist, lg, "circom", 200 + k) for k, lg in enumerate(logs)]
+    t_tune = time.perf_counter()
+    tuned = autotune_sizes(args, api, ctx, logs, api.SKEWED)
+    t_tune = time.perf_counter() - t_tune
     circuits = [api.Circuit(z, ctx=ctx) for z, _ in files]
+    wits = [api.read_wtns(w) for _, w in files]
     t = time.perf_counter()
-    for c in circuits:
+    for c, w in zip(circuits, wits):
+        c.prove(w)  # detects the witness distribution (keys the tuned settings)
         c.precompute(0, 0)
     t_pre = time.perf_counter() - t
-    wits = [api.read_wtns(w) for _, w in files]
     alone = [c.prove(w) for c, w in zip(circuits, wits)]  # the reference answer per circuit
 
     def leg(rate, seconds, seed):
@@ -468,7 +545,7 @@ def run_serving(args, dist, ctx, L):
                 tk, k = item
                 try:
                     p, ms = srv.wait(tk)
-                    lat.append(ms)
+                    lat.append((k, ms))
                     done[0] += 1
                     if not np.array_equal(p, alone[k]):
                         bad[0] += 1
@@ -500,7 +577,13 @@ def run_serving(args, dist, ctx, L):
         return {"offered_req_per_s": rate, "seconds": round(window, 2), "submitted": sent,
                 "completed": done[0], "dropped_unstarted": dropped[0],
                 "sustained_proofs_per_s": done[0] / (time.perf_counter() - t0),
-                "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
+                "latency_ms": {"p50": pct([m for _, m in lat], 50),
+                               "p99": pct([m for _, m in lat], 99)},
+                "latency_ms_by_size": {
+                    f"2^{logs[q]}": {"n": sum(1 for k, _ in lat if k == q),
+                                     "p50": pct([m for k, m in lat if k == q], 50),
+                                     "p99": pct([m for k, m in lat if k == q], 99)}
+                    for q in range(4)},
                 "peak_inflight": st["peak_inflight"], "admission_waits": st["admission_waits"],
                 "mismatches": bad[0]}
 
@@ -514,7 +597,8 @@ def run_serving(args, dist, ctx, L):
                         f"2^{logs[3]} mixed 50/25/15/10, circom-like witnesses, resident CRS "
                         f"with fixed-base tables (built in {t_pre:.1f} s)",
             "server": f"zk_server, up to {args.serve_inflight} proofs in flight, "
-                      "admission by free device memory",
+                      "admission by free device memory, smallest circuit first with aging",
+            "autotuned": tuned, "autotune_s": round(t_tune, 1),
             "at_offered_rate": over, "at_80pct_of_sustained": fair, "bit_exact": True}
 
 

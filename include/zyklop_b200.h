@@ -218,6 +218,21 @@ int zk_prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* circuits,
  * kernels and copies across 5 streams) into a CUDA graph the first time it
  * proves a circuit and replays it afterwards.  Results are unchanged. */
 int zk_ctx_set_graphs(zk_ctx* ctx, int on);
+/* How zk_prove_batch runs: mode 1 = in-flight pipelines (up to `inflight`
+ * proofs at once, each with its own workspace and streams); mode 2 = fused
+ * groups: proofs over circuits with fixed-base tables (zk_circuit_precompute)
+ * are grouped by table window bits, up to `group` per group, and each group
+ * runs two multi-instance MSM launch chains (every job's G1 MSMs in one,
+ * every job's B2 in the other) after per-job SpMV / H, with two groups
+ * alternating so host combination overlaps GPU work; mode 0 (default) =
+ * fused when every circuit has tables, else in-flight.  Results never
+ * change. */
+int zk_ctx_set_batch_mode(zk_ctx* ctx, int mode, int group);
+/* Streams a proof spreads its MSMs over (1..5; 0 = the default 5, or the
+ * ZYKLOP_PROVE_STREAMS environment variable).  With 1 the MSMs run back to
+ * back, so per-kernel timings (zk_ctx_profile) are not shared with other
+ * kernels of the same proof.  Results never change. */
+int zk_ctx_set_prove_streams(zk_ctx* ctx, int n);
 
 /* Autotuning.  Each call times candidate settings on seeded synthetic inputs
  * (points k_i * G, scalars of the given distribution: 0 uniform in Fr, 1 the

@@ -423,3 +423,61 @@ def test_server_admits_small_circuits_first(api, files):
             assert done[4] < done[3]
         else:
             assert done[4] > done[3]
+
+
+@pytest.mark.parametrize("group", [3, 16])
+def test_fused_batch_matches_single_proofs(api, oracle, files, group):
+    """Fused groups (multi-instance MSM chains over several proofs) give,
+    job for job, the single-proof results: mixed circuits and table sizes,
+    several groups with alternating workspaces, blinded and unblinded."""
+    names = ["u10", "c10", "u16", "u10", "c10", "c10", "u16", "u10", "c10", "u10", "c10", "u16",
+             "u10"]
+    circ = {}
+    for nm in ("u10", "c10", "u16"):
+        circ[nm] = api.Circuit(files[nm][0])
+    circ["u10"].precompute(10, 9)   # u10 and c10 share table bits (one group key) ...
+    circ["c10"].precompute(10, 9)
+    circ["u16"].precompute(12, 11)  # ... u16 forms its own
+    wits = {nm: api.read_wtns(files[nm][1]) for nm in circ}
+    single = {nm: circ[nm].prove(wits[nm]) for nm in circ}
+    try:
+        api.set_batch_mode(api.BATCH_FUSED, group)
+        proofs = api.prove_batch([circ[nm] for nm in names], [wits[nm] for nm in names])
+        for k, nm in enumerate(names):
+            assert np.array_equal(proofs[k], single[nm]), (k, nm)
+        rs = [5 + 3 * k for k in range(5)]
+        ss = [7 + 11 * k for k in range(5)]
+        sub = names[:5]
+        bp = api.prove_batch([circ[nm] for nm in sub], [wits[nm] for nm in sub], rs=rs, ss=ss)
+        for k, nm in enumerate(sub):
+            z, w = files[nm]
+            assert np.array_equal(bp[k], oracle.prove(blob(z), blob(w), r=rs[k], s=ss[k])), (k, nm)
+        # device witnesses
+        dw = [api.to_device(wits[nm]) for nm in names[:4]]
+        from zyklop_b200._lib import check, lib
+        handles = (ctypes.c_void_p * 4)(*[circ[nm].handle.value for nm in names[:4]])
+        wp = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in dw])
+        nw = (ctypes.c_size_t * 4)(*[t.numel() // 4 for t in dw])
+        out = np.zeros((4, 32), np.uint64)
+        check(lib().zk_prove_batch(None, 4, handles, wp, nw, 1, None, None,
+                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 1))
+        for k, nm in enumerate(names[:4]):
+            assert np.array_equal(out[k], single[nm]), (k, nm)
+    finally:
+        api.set_batch_mode(api.BATCH_AUTO, 16)
+    for c in circ.values():
+        c.close()
+
+
+def test_fused_batch_needs_tables(api, files):
+    from zyklop_b200 import ZkError
+    c = api.Circuit(files["u10"][0])
+    wit = api.read_wtns(files["u10"][1])
+    try:
+        api.set_batch_mode(api.BATCH_FUSED, 8)
+        with pytest.raises(ZkError) as e:
+            api.prove_batch([c], [wit])
+        assert e.value.code == 1
+    finally:
+        api.set_batch_mode(api.BATCH_AUTO, 16)
+    assert np.array_equal(api.prove_batch([c], [wit])[0], c.prove(wit))

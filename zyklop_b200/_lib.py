@@ -74,6 +74,8 @@ SIGNATURES = {
                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                       ctypes.c_void_p, u64p, ctypes.c_int]),
     "zk_ctx_set_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "zk_ctx_set_prove_streams": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "zk_ctx_set_batch_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "zk_autotune_msm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_void_p]),
     "zk_autotune_table_c": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,

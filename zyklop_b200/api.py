@@ -303,8 +303,22 @@ def set_graphs(on, ctx=None):
     check(lib().zk_ctx_set_graphs(ctx, 1 if on else 0))
 
 
+BATCH_AUTO, BATCH_INFLIGHT, BATCH_FUSED = 0, 1, 2
+
+
+def set_batch_mode(mode, group=16, ctx=None):
+    """0: fused when every circuit has tables, else in-flight; 1: in-flight
+    pipelines; 2: fused groups of up to `group` proofs"""
+    check(lib().zk_ctx_set_batch_mode(ctx, mode, group))
+
+
 # ------------------------------------------------------------- autotuning
 UNIFORM, SKEWED = 0, 1
+
+
+def table_c_default(log_n):
+    """fixed-base window bits used when nothing is tuned for the size"""
+    return min(max(log_n, 8), 20)
 
 
 def autotune_msm(group, log_n, dist=UNIFORM, fixed_c=0, ctx=None):

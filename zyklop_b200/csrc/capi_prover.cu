@@ -174,7 +174,36 @@ int zk_prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* circuits,
   ZK_REQUIRE((r == nullptr) == (s == nullptr), ZK_EINVAL, "zk_prove_batch: give both r and s or neither");
   ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
-  prove_batch(ctx, count, circuits, witnesses, n_witness, on_device != 0, r, s, proofs, inflight);
+  bool fused = ctx->batch_mode == 2;
+  if (ctx->batch_mode == 0) {  // auto: fused when every circuit has fixed-base tables
+    fused = count > 0 && circuits;
+    for (size_t i = 0; fused && i < count; i++) fused = circuits[i] && circuits[i]->tab_c[0] != 0;
+  }
+  if (fused)
+    prove_batch_fused(ctx, count, circuits, witnesses, n_witness, on_device != 0, r, s, proofs,
+                      ctx->batch_group);
+  else
+    prove_batch(ctx, count, circuits, witnesses, n_witness, on_device != 0, r, s, proofs, inflight);
+  ZK_API_END
+}
+
+int zk_ctx_set_prove_streams(zk_ctx* ctx, int n) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(n >= 0 && n <= zk::ProveWs::kStreams, ZK_EINVAL, "zk_ctx_set_prove_streams: 0..5");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->prove_streams = n;
+  ZK_API_END
+}
+
+int zk_ctx_set_batch_mode(zk_ctx* ctx, int mode, int group) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(mode >= 0 && mode <= 2, ZK_EINVAL, "zk_ctx_set_batch_mode: mode 0, 1 or 2");
+  ZK_REQUIRE(group >= 1 && group <= 64, ZK_EINVAL, "zk_ctx_set_batch_mode: group 1..64");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->batch_mode = mode;
+  ctx->batch_group = group;
   ZK_API_END
 }
 

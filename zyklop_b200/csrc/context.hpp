@@ -23,7 +23,8 @@ constexpr size_t kMaxWindowBytes = 2 * 64 * 256;
 struct ProveWs {
   static constexpr int kStreams = 5;  // 0: witness/SpMV/H/MSM_H, 1: A, 2: B2, 3: C, 4: B1
   bool ready = false;
-  int nstreams = kStreams;
+  int nstreams = kStreams;      // streams the current proof spreads its MSMs over
+  int env_nstreams = kStreams;  // ZYKLOP_PROVE_STREAMS, else kStreams
   cudaStream_t st[kStreams] = {};
   cudaEvent_t ev_we = nullptr, ev_begin = nullptr, ev_all = nullptr;
   cudaEvent_t ev_done[kStreams] = {};
@@ -40,6 +41,7 @@ struct ProveWs {
     bool blind = false;
     int ntt_lmax = 0;  // twiddle table the graph reads
     int ntt_bits = 0;  // NTT pass radix captured
+    int nstreams = 0;  // MSM streams captured
     MsmConfig cfg[kStreams];  // settings of each MSM captured
     int tab_c[2] = {0, 0};  // fixed-base table windows captured (0: windowed)
     uint64_t kernels = 0;
@@ -51,6 +53,22 @@ struct ProveWs {
   void drop_graph();
   cudaEvent_t ev_begin_pool() { init(); return ev_begin; }
   ~ProveWs();
+};
+
+// Workspace of one fused batch group (see prove_batch_fused): streams, every
+// job's witness and polynomial buffers, the two multi-instance MSM arenas and
+// their pinned result copies.
+struct FusedWs {
+  static constexpr int kPolyStreams = 4;
+  bool ready = false;
+  // s1: staging, then the H chain; s2: the B2 chain; s3: the A / C / B1
+  // chain; sp[]: SpMV and H polynomials of the jobs, round robin
+  cudaStream_t s1 = nullptr, s2 = nullptr, s3 = nullptr, sp[kPolyStreams] = {};
+  cudaEvent_t ev_staged = nullptr, ev_g2 = nullptr, ev_g1w = nullptr, ev_done = nullptr;
+  cudaEvent_t ev_sp[kPolyStreams] = {};
+  DeviceBuffer we, poly, g1w, gh, g2;
+  PinnedBuffer win1w, winh, win2;
+  ~FusedWs();
 };
 
 }  // namespace zk
@@ -66,8 +84,12 @@ struct zk_ctx {
   zk::TuneTable tune;             // autotuned settings
   int scalar_dist = 0;            // distribution hint for zk_msm_g1 / g2
   zk::ProveWs ws;
-  std::vector<std::unique_ptr<zk::ProveWs>> pool;  // batch workspaces
+  std::vector<std::unique_ptr<zk::ProveWs>> pool;  // in-flight batch workspaces
+  zk::FusedWs fused[2];                            // fused batch groups (alternating)
+  int batch_mode = 0;    // 0 auto, 1 in-flight pipelines, 2 fused groups
+  int batch_group = 16;  // proofs per fused group
   bool use_graphs = false;  // replay captured per-circuit proof graphs
+  int prove_streams = 0;    // MSM streams per proof (0: ZYKLOP_PROVE_STREAMS or 5)
   zk::Stager stager;
   zk::Profiler prof;
   bool profiling = false;

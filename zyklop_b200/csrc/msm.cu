@@ -24,8 +24,10 @@ constexpr int kRedT = 128;  // pairs per block in the bucket-reduction block pas
 struct Shape {
   size_t n;
   int c, W;              // window bits, scalar windows
-  int Wk;                // bucket sets: W, or 1 when windows share buckets (fixed bases)
+  int Wk;                // bucket sets: W, or one per instance when windows share buckets
+                         // (fixed bases)
   bool fixed;            // points carry precomputed 2^(c w) multiples (table of W*n records)
+  int inst;              // fixed-base instances sharing the launch (1 otherwise)
   uint32_t B;            // buckets per set (2^(c-1))
   size_t entries;        // W*B + 1 scan entries (last = total)
   size_t records;        // W*n upper bound on sorted records
@@ -36,16 +38,18 @@ struct Shape {
   size_t J;              // bucket-reduction level-1 chunks per window
 };
 
-Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false) {
+// n: points (summed over instances for fixed-base multi-instance MSMs)
+Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false, int inst = 1) {
   const int seg_t = g2 ? 64 : 128;
   Shape s{};
   s.n = n;
+  s.inst = fixed ? inst : 1;
   s.c = cfg.c > 0 ? cfg.c : msm_default_c(n, g2);
   // the top window holds < c bits, so no carry leaves it; fixed-base MSMs
   // reduce scalars mod r first (254 bits)
   s.fixed = fixed;
   s.W = (fixed ? 254 : 256) / s.c + 1;
-  s.Wk = fixed ? 1 : s.W;
+  s.Wk = fixed ? s.inst : s.W;
   s.B = 1u << (s.c - 1);
   s.entries = (size_t)s.Wk * s.B + 1;
   s.records = std::max<size_t>((size_t)s.W * n, 1);
@@ -173,21 +177,33 @@ __device__ __forceinline__ void reduce_mod_r(uint32_t s[8]) {
   }
 }
 
-// kFixed: all windows share one bucket set, and the record value names the
-// table entry (window w of point i: w * n + i) instead of the point.
+// Scalar sources of one launch.  Windowed MSMs: one instance, key
+// w * B + bucket, record value = point index.  Fixed-base MSMs: up to
+// kMaxInst instances (grid.y), each with its own scalars and table; all
+// windows of an instance share its bucket set, key = instance * B + bucket,
+// and the record value names the instance's table entry (window w of point
+// i: w * n + i).
+constexpr int kMaxInst = 64;
+struct ScalarSrc {
+  const uint64_t* sc[kMaxInst];
+  uint32_t n[kMaxInst];
+};
+
 template <bool kFixed>
-__global__ void k_msm_hist(const uint64_t* __restrict__ sc, size_t n, int c, int W, uint32_t B,
+__global__ void k_msm_hist(const __grid_constant__ ScalarSrc src, int c, int W, uint32_t B,
                            uint32_t* __restrict__ counts) {
+  const int inst = blockIdx.y;
+  const uint32_t n = src.n[inst];
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i < n;
   uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (active) load_scalar(sc, i, s);
+  if (active) load_scalar(src.sc[inst], i, s);
   if (kFixed) reduce_mod_r(s);
   const int lane = threadIdx.x & 31;
   uint32_t carry = 0;
   for (int w = 0; w < W; w++) {
     bool neg;
-    uint32_t key = next_digit(s, c, B, kFixed ? 0 : w, carry, neg);
+    uint32_t key = next_digit(s, c, B, kFixed ? inst : w, carry, neg);
     if (!active) key = kInvalid;
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     if (key != kInvalid && lane == __ffs(peers) - 1) atomicAdd(&counts[key], (uint32_t)__popc(peers));
@@ -195,20 +211,22 @@ __global__ void k_msm_hist(const uint64_t* __restrict__ sc, size_t n, int c, int
 }
 
 template <bool kFixed>
-__global__ void k_msm_scatter(const uint64_t* __restrict__ sc, size_t n, int c, int W, uint32_t B,
+__global__ void k_msm_scatter(const __grid_constant__ ScalarSrc src, int c, int W, uint32_t B,
                               uint32_t* __restrict__ cursor, uint32_t* __restrict__ skey,
                               uint32_t* __restrict__ sval) {
+  const int inst = blockIdx.y;
+  const uint32_t n = src.n[inst];
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = i < n;
   uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (active) load_scalar(sc, i, s);
+  if (active) load_scalar(src.sc[inst], i, s);
   if (kFixed) reduce_mod_r(s);
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   uint32_t carry = 0;
   for (int w = 0; w < W; w++) {
     bool neg;
-    uint32_t key = next_digit(s, c, B, kFixed ? 0 : w, carry, neg);
+    uint32_t key = next_digit(s, c, B, kFixed ? inst : w, carry, neg);
     if (!active) key = kInvalid;
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     const int leader = __ffs(peers) - 1;
@@ -344,12 +362,21 @@ __device__ __forceinline__ void seg_block_finish(SegNode<F>* sm, uint32_t key_be
   }
 }
 
-// Level 0: records are (bucket key, point index | sign) in bucket order.
+// Where level 0 reads the points of its records.
 template <class F>
+struct PointSrc {
+  const F* x;  // windowed: point i at x + i * stride, y likewise
+  const F* y;
+  uint32_t stride;
+  int bshift;                 // fixed-base: instance = key >> bshift
+  const F* table[kMaxInst];   // fixed-base: record r of an instance at table + 2 r (x, y)
+};
+
+// Level 0: records are (bucket key, point index | sign) in bucket order.
+template <class F, bool kFixed>
 __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
-    const uint32_t* __restrict__ total_p, const F* __restrict__ px, const F* __restrict__ py,
-    uint32_t pstride, int K,
+    const uint32_t* __restrict__ total_p, const __grid_constant__ PointSrc<F> src, int K,
     xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
   constexpr int T = seg_threads<F>();
   __shared__ SegNode<F> sm[T];
@@ -376,8 +403,15 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
       }
       const uint32_t v = sval[p];
       const uint32_t idx = v & ~kNeg;
-      const F x = ld_pod(px + (size_t)idx * pstride);
-      F y = ld_pod(py + (size_t)idx * pstride);
+      F x, y;
+      if (kFixed) {
+        const F* t = src.table[key >> src.bshift];
+        x = ld_pod(t + 2 * (size_t)idx);
+        y = ld_pod(t + 2 * (size_t)idx + 1);
+      } else {
+        x = ld_pod(src.x + (size_t)idx * src.stride);
+        y = ld_pod(src.y + (size_t)idx * src.stride);
+      }
       if (!(fe_is_zero(x) && fe_is_zero(y))) {
         if (v & kNeg) y = fe_neg(y);
         acc = xyzz_madd(acc, x, y);
@@ -547,50 +581,55 @@ __global__ void __launch_bounds__(128) k_msm_precompute(const F* __restrict__ px
 }
 
 
+// The GPU part of one launch chain: a windowed MSM (inst = 1, points from
+// ps.x / ps.y) or inst fixed-base MSMs of one window size sharing the chain
+// (tables in ps.table).  n_max: the largest instance, n_total: their sum.
 template <class F>
-MsmResult msm_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                      size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t st,
-                      bool fixed = false) {
+MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size_t n_max,
+                      size_t n_total, void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
+                      cudaStream_t st, bool fixed) {
   constexpr bool g2 = sizeof(F) == 64;
-  ZK_REQUIRE(n < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
-  const Shape s = make_shape(n, g2, cfg, fixed);
-  ZK_REQUIRE(!fixed || (size_t)s.W * n < (size_t(1) << 31), ZK_EINVAL,
+  ZK_REQUIRE(n_max < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
+  ZK_REQUIRE(inst >= 1 && inst <= kMaxInst, ZK_EINVAL, "msm: 1..64 instances per launch");
+  const Shape s = make_shape(n_total, g2, cfg, fixed, inst);
+  ZK_REQUIRE(!fixed || (size_t)s.W * n_max < (size_t(1) << 31), ZK_EINVAL,
              "msm: fixed-base table too large (windows x points >= 2^31)");
   ZK_REQUIRE(s.c >= 4 && s.c <= 24, ZK_EINVAL, "msm: window size must be in [4, 24]");
   ZK_REQUIRE(s.records < (size_t(1) << 32) - 1, ZK_EINVAL, "msm: too many (point, window) records");
+  ZK_REQUIRE(!fixed || (size_t)inst * s.B < kInvalid, ZK_EINVAL, "msm: too many buckets");
   Layout<F> L = carve<F>(scratch, s);
   ZK_REQUIRE(L.bytes <= scratch_bytes, ZK_EINVAL, "msm: scratch buffer too small");
 
   ZK_CUDA(cudaMemsetAsync(L.counts, 0, s.entries * sizeof(uint32_t), st));
   ZK_CUDA(cudaMemsetAsync(L.buckets, 0, (size_t)s.Wk * s.B * sizeof(xyzz<F>), st));
-  if (n) {
-    const int th = 256;
-    const unsigned g = (unsigned)((n + th - 1) / th);
+  const int th = 256;
+  const dim3 g((unsigned)((n_max + th - 1) / th), (unsigned)inst);
+  if (n_max) {
     if (fixed)
-      k_msm_hist<true><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
+      k_msm_hist<true><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.counts);
     else
-      k_msm_hist<false><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.counts);
+      k_msm_hist<false><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.counts);
     ZK_LAUNCHED();
   }
   scan::exclusive(L.counts, L.cursor, s.entries, L.tiles, st);
-  if (n) {
-    const int th = 256;
-    const unsigned g = (unsigned)((n + th - 1) / th);
+  if (n_max) {
     if (fixed)
-      k_msm_scatter<true><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
+      k_msm_scatter<true><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
     else
-      k_msm_scatter<false><<<g, th, 0, st>>>(scalars, n, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
+      k_msm_scatter<false><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
     ZK_LAUNCHED();
   }
   const uint32_t* total_p = L.counts + (s.entries - 1);
-  const F* fx = reinterpret_cast<const F*>(pts.x);
-  const F* fy = reinterpret_cast<const F*>(pts.y);
   // level 0
   {
     uint32_t* ok = s.levels > 1 ? L.pkey[1] : nullptr;
-    ProfScope prof(g2 ? kProfAccumG2 : kProfAccumG1, (double)n, st);
-    k_msm_accum0<F><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
-        L.skey, L.sval, total_p, fx, fy, pts.stride, s.k0, L.buckets, ok, L.ppt[1]);
+    ProfScope prof(g2 ? kProfAccumG2 : kProfAccumG1, (double)n_total, st);
+    if (fixed)
+      k_msm_accum0<F, true><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
+          L.skey, L.sval, total_p, ps, s.k0, L.buckets, ok, L.ppt[1]);
+    else
+      k_msm_accum0<F, false><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
+          L.skey, L.sval, total_p, ps, s.k0, L.buckets, ok, L.ppt[1]);
     ZK_LAUNCHED();
   }
   for (int l = 1; l < s.levels; l++) {
@@ -653,10 +692,10 @@ size_t msm_table_bytes(size_t n, bool g2, int c) {
   return (size_t)(254 / c + 1) * n * (g2 ? 128 : 64);
 }
 
-size_t msm_scratch_bytes_fixed(size_t n, bool g2, int c, const MsmConfig& cfg) {
+size_t msm_scratch_bytes_fixed(size_t n, bool g2, int c, const MsmConfig& cfg, int inst) {
   MsmConfig k = cfg;
   k.c = c;
-  const Shape s = make_shape(n, g2, k, true);
+  const Shape s = make_shape(n, g2, k, true, inst);
   if (g2) return carve<fp2_t>(nullptr, s).bytes;
   return carve<fp_t>(nullptr, s).bytes;
 }
@@ -677,22 +716,63 @@ void msm_precompute(bool g2, const PointsView& pts, size_t n, int c, void* table
   ZK_LAUNCHED();
 }
 
-MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
-                            void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
+namespace {
+template <class F>
+MsmResult enqueue_fixed_multi(int inst, const void* const* tables, const uint64_t* const* scalars,
+                              const size_t* n, int c, void* scratch, size_t bytes,
+                              const MsmConfig& cfg, cudaStream_t st) {
+  ZK_REQUIRE(inst >= 1 && inst <= kMaxInst, ZK_EINVAL, "msm: 1..64 instances per launch");
   MsmConfig k = cfg;
   k.c = c;
-  const PointsView pts = points_aos(table, g2);
-  if (g2) return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, k, st, true);
-  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, k, st, true);
+  ScalarSrc ss{};
+  PointSrc<F> ps{};
+  ps.bshift = c - 1;
+  size_t n_max = 0, n_total = 0;
+  for (int i = 0; i < inst; i++) {
+    ZK_REQUIRE(n[i] < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
+    ss.sc[i] = scalars[i];
+    ss.n[i] = (uint32_t)n[i];
+    ps.table[i] = reinterpret_cast<const F*>(tables[i]);
+    n_max = std::max(n_max, n[i]);
+    n_total += n[i];
+  }
+  return msm_enqueue<F>(ss, ps, inst, n_max, n_total, scratch, bytes, k, st, true);
+}
+
+template <class F>
+MsmResult enqueue_windowed(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
+                           size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
+  ScalarSrc ss{};
+  ss.sc[0] = scalars;
+  ss.n[0] = (uint32_t)std::min(n, size_t(0xffffffffu));
+  PointSrc<F> ps{};
+  ps.x = reinterpret_cast<const F*>(pts.x);
+  ps.y = reinterpret_cast<const F*>(pts.y);
+  ps.stride = pts.stride;
+  return msm_enqueue<F>(ss, ps, 1, n, n, scratch, bytes, cfg, st, false);
+}
+}  // namespace
+
+MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
+                            void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
+  return msm_enqueue_fixed_multi(g2, 1, &table, &scalars, &n, c, scratch, bytes, cfg, st);
+}
+
+MsmResult msm_enqueue_fixed_multi(bool g2, int inst, const void* const* tables,
+                                  const uint64_t* const* scalars, const size_t* n, int c,
+                                  void* scratch, size_t bytes, const MsmConfig& cfg,
+                                  cudaStream_t st) {
+  if (g2) return enqueue_fixed_multi<fp2_t>(inst, tables, scalars, n, c, scratch, bytes, cfg, st);
+  return enqueue_fixed_multi<fp_t>(inst, tables, scalars, n, c, scratch, bytes, cfg, st);
 }
 
 MsmResult msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
                          size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
-  return msm_enqueue<fp_t>(pts, scalars, n, scratch, bytes, cfg, st);
+  return enqueue_windowed<fp_t>(pts, scalars, n, scratch, bytes, cfg, st);
 }
 MsmResult msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
                          size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
-  return msm_enqueue<fp2_t>(pts, scalars, n, scratch, bytes, cfg, st);
+  return enqueue_windowed<fp2_t>(pts, scalars, n, scratch, bytes, cfg, st);
 }
 
 namespace {
@@ -718,6 +798,30 @@ host::Xyzz<T> combine(const uint8_t* data, const MsmResult& r, size_t pt_bytes, 
   return acc;
 }
 }  // namespace
+
+// instance i of a multi-instance result: its (U_i, A_i) as a one-window result
+MsmResult gather_instance(const void* h_data, const MsmResult& r, int inst, size_t pt_bytes,
+                          uint8_t* buf) {
+  const uint8_t* d = reinterpret_cast<const uint8_t*>(h_data);
+  memcpy(buf, d + (size_t)inst * pt_bytes, pt_bytes);
+  memcpy(buf + pt_bytes, d + (size_t)(r.windows + inst) * pt_bytes, pt_bytes);
+  MsmResult one = r;
+  one.windows = 1;
+  one.bytes = 2 * pt_bytes;
+  return one;
+}
+
+bool msm_g1_combine_inst(const void* h_data, const MsmResult& r, int inst, uint64_t out[8]) {
+  alignas(16) uint8_t buf[256];
+  const MsmResult one = gather_instance(h_data, r, inst, 128, buf);
+  return msm_g1_combine(buf, one, out);
+}
+
+bool msm_g2_combine_inst(const void* h_data, const MsmResult& r, int inst, uint64_t out[16]) {
+  alignas(16) uint8_t buf[512];
+  const MsmResult one = gather_instance(h_data, r, inst, 256, buf);
+  return msm_g2_combine(buf, one, out);
+}
 
 bool msm_g1_combine(const void* h_data, const MsmResult& r, uint64_t out[8]) {
   using P = host::Xyzz<host::Fp>;

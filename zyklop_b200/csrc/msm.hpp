@@ -85,17 +85,30 @@ MsmResult msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t 
 // returns a single window sum (combine it with n_windows = 1).  Scalars are
 // reduced mod r first, which requires points of order r (CRS points are).
 size_t msm_table_bytes(size_t n, bool g2, int c);
-size_t msm_scratch_bytes_fixed(size_t n, bool g2, int c, const MsmConfig& cfg);
+size_t msm_scratch_bytes_fixed(size_t n, bool g2, int c, const MsmConfig& cfg, int inst = 1);
 void msm_precompute(bool g2, const PointsView& pts, size_t n, int c, void* table,
                     cudaStream_t stream);
 MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
                             void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
                             cudaStream_t stream);
+// Several fixed-base MSMs with the same window bits in one launch chain: one
+// instance per (table, scalars, n); their records share the sort, the
+// load-balanced accumulation and the bucket reduction (instance i's buckets
+// take the place of window i).  Scratch: msm_scratch_bytes_fixed(sum of n,
+// g2, c, cfg, inst).  The result holds one window sum per instance
+// (msm_g*_combine_inst).
+constexpr int kMsmMaxInstances = 64;
+MsmResult msm_enqueue_fixed_multi(bool g2, int inst, const void* const* tables,
+                                  const uint64_t* const* scalars, const size_t* n, int c,
+                                  void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
+                                  cudaStream_t stream);
 
 // Host combination of an MSM result (r.bytes copied from r.d_data) into an
 // affine Montgomery point.  Returns true for the point at infinity.
 bool msm_g1_combine(const void* h_data, const MsmResult& r, uint64_t out[8]);
 bool msm_g2_combine(const void* h_data, const MsmResult& r, uint64_t out[16]);
+bool msm_g1_combine_inst(const void* h_data, const MsmResult& r, int inst, uint64_t out[8]);
+bool msm_g2_combine_inst(const void* h_data, const MsmResult& r, int inst, uint64_t out[16]);
 
 // Blocking convenience wrappers: enqueue, copy the window sums back, combine.
 bool msm_g1_run(const PointsView& pts, const uint64_t* scalars, size_t n, DeviceBuffer& scratch,

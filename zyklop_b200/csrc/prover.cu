@@ -116,7 +116,7 @@ void ProveWs::init() {
   // (a tuning knob: concurrent MSMs share L2 and the SMs)
   if (const char* e = getenv("ZYKLOP_PROVE_STREAMS")) {
     const int v = atoi(e);
-    if (v >= 1 && v <= kStreams) nstreams = v;
+    if (v >= 1 && v <= kStreams) env_nstreams = v;
   }
   for (int i = 0; i < kStreams; i++) {
     ZK_CUDA(cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking));
@@ -295,6 +295,7 @@ void ws_scratch_needs(zk_circuit* c, bool blind, const MsmConfig cfg[ProveWs::kS
 void ws_prepare(zk_circuit* c, ProveWs& ws, bool blind) {
   zk_ctx* ctx = c->ctx;
   ws.init();
+  ws.nstreams = ctx->prove_streams ? ctx->prove_streams : ws.env_nstreams;
   const size_t m1 = c->m1, n = c->n;
   ws_msm_configs(c, ws.cfg);
   size_t need[ProveWs::kStreams];
@@ -369,20 +370,7 @@ void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg
   launch(3, false, c->pts_c, c->tab_c_pts, we + 4 * (l + 2), nc);
   if (blind) launch(4, false, c->pts_b1, c->tab_b1, we, m1 + 1);
 
-  SpmvArgs sa;
-  for (int m = 0; m < 2; m++) {
-    sa.row[m] = c->row[m].as<uint32_t>();
-    sa.sig[m] = c->sig[m].as<uint32_t>();
-    sa.val[m] = c->val[m].as<fr_t>();
-  }
-  sa.out[0] = ws.aw.as<fr_t>();
-  sa.out[1] = ws.bw.as<fr_t>();
-  {
-    ProfScope prof(kProfSpmv, (double)c->n_coefs, s0);
-    k_spmv<<<dim3(blocks(n, 256), 2), 256, 0, s0>>>(sa, reinterpret_cast<const fr_t*>(we + 4),
-                                                    (uint32_t)n);
-    ZK_LAUNCHED();
-  }
+  spmv_enqueue(c, we, ws.aw.as<uint64_t>(), ws.bw.as<uint64_t>(), s0);
   if (dbg && (dbg->aw || dbg->bw)) {
     if (dbg->aw) ZK_CUDA(cudaMemcpyAsync(dbg->aw, ws.aw.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
     if (dbg->bw) ZK_CUDA(cudaMemcpyAsync(dbg->bw, ws.bw.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
@@ -410,6 +398,7 @@ void ws_launch(zk_circuit* c, ProveWs& ws, bool blind, bool use_graph, ProveInte
   ProveWs::Graph* gr = nullptr;
   for (ProveWs::Graph& x : ws.graphs)
     if (x.circuit == c->id && x.blind == blind && x.ntt_lmax == lmax && x.ntt_bits == bits &&
+        x.nstreams == ws.nstreams &&
         same_cfg(x) && x.tab_c[0] == c->tab_c[0] && x.tab_c[1] == c->tab_c[1])
       gr = &x;
   if (!gr) {
@@ -441,6 +430,7 @@ void ws_launch(zk_circuit* c, ProveWs& ws, bool blind, bool use_graph, ProveInte
     x.blind = blind;
     x.ntt_lmax = lmax;
     x.ntt_bits = bits;
+    x.nstreams = ws.nstreams;
     for (int i = 0; i < ProveWs::kStreams; i++) x.cfg[i] = ws.cfg[i];
     x.tab_c[0] = c->tab_c[0];
     x.tab_c[1] = c->tab_c[1];
@@ -463,10 +453,33 @@ void ws_finish(zk_circuit* c, ProveWs& ws, bool blind, const uint64_t* r, const 
   msm_g2_combine(ws.win[2].ptr, ws.res[2], pb);
   msm_g1_combine(ws.win[3].ptr, ws.res[3], pc);
   msm_g1_combine(ws.win[0].ptr, ws.res[0], ph);
+  if (blind) msm_g1_combine(ws.win[4].ptr, ws.res[4], pb1);
+  assemble_proof(c, pa, pb, pc, ph, blind ? pb1 : nullptr, r, s, proof);
+}
+
+}  // namespace
+
+void spmv_enqueue(zk_circuit* c, const uint64_t* we, uint64_t* aw, uint64_t* bw, cudaStream_t st) {
+  SpmvArgs sa;
+  for (int m = 0; m < 2; m++) {
+    sa.row[m] = c->row[m].as<uint32_t>();
+    sa.sig[m] = c->sig[m].as<uint32_t>();
+    sa.val[m] = c->val[m].as<fr_t>();
+  }
+  sa.out[0] = reinterpret_cast<fr_t*>(aw);
+  sa.out[1] = reinterpret_cast<fr_t*>(bw);
+  ProfScope prof(kProfSpmv, (double)c->n_coefs, st);
+  k_spmv<<<dim3(blocks(c->n, 256), 2), 256, 0, st>>>(sa, reinterpret_cast<const fr_t*>(we + 4),
+                                                     (uint32_t)c->n);
+  ZK_LAUNCHED();
+}
+
+void assemble_proof(const zk_circuit* c, const uint64_t pa[8], const uint64_t pb[16],
+                    const uint64_t pc[8], const uint64_t ph[8], const uint64_t* pb1,
+                    const uint64_t* r, const uint64_t* s, uint64_t proof[32]) {
   G1 A = g1_aff(pa), Cc = g1_aff(pc).add(g1_aff(ph));
   G2 B = g2_aff(pb);
-  if (blind) {
-    msm_g1_combine(ws.win[4].ptr, ws.res[4], pb1);
+  if (pb1) {
     const G1 d1 = g1_aff(c->delta1);
     A = A.add(mul(d1, r));
     B = B.add(mul(g2_aff(c->delta2), s));
@@ -493,7 +506,6 @@ void note_witness(zk_circuit* c, const uint64_t* witness, bool on_device) {
   if (c->dist_auto && !on_device) c->dist = detect_scalar_dist(witness, c->m1);
 }
 
-}  // namespace
 
 // Device bytes that preparing ws for this circuit would newly allocate (the
 // proof server admits a request only when that much memory is free).

@@ -85,6 +85,27 @@ void prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* cs, const uint64_
                  const size_t* nwits, bool on_device, const uint64_t* rs, const uint64_t* ss,
                  uint64_t* proofs, int inflight);
 
+// Fused batches: jobs whose circuits hold fixed-base tables are grouped by
+// table window bits; each group of up to `group` proofs runs as one launch
+// chain per stage (witness staging, SpMV and H per job, then one
+// multi-instance G1 MSM over every job's A / C / H (/ B1) and one over every
+// job's B2), and two group workspaces alternate so one group's host
+// combination overlaps the next group's GPU work.
+void prove_batch_fused(zk_ctx* ctx, size_t count, zk_circuit* const* cs,
+                       const uint64_t* const* wits, const size_t* nwits, bool on_device,
+                       const uint64_t* rs, const uint64_t* ss, uint64_t* proofs, int group);
+
+// Pieces shared by the single, in-flight and fused paths.
+void check_job(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool blind);
+void note_witness(zk_circuit* c, const uint64_t* witness, bool on_device);
+// A.w, B.w (Montgomery, domain entries each) from we = [1 || w] on `st`.
+void spmv_enqueue(zk_circuit* c, const uint64_t* we, uint64_t* aw, uint64_t* bw, cudaStream_t st);
+// pi_A, pi_B, pi_C from the MSM sums (affine Montgomery); pb1 (the B1 MSM),
+// r and s are null for the unblinded proof.
+void assemble_proof(const zk_circuit* c, const uint64_t pa[8], const uint64_t pb[16],
+                    const uint64_t pc[8], const uint64_t ph[8], const uint64_t* pb1,
+                    const uint64_t* r, const uint64_t* s, uint64_t proof[32]);
+
 uint64_t next_circuit_id();
 
 }  // namespace zk

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <sstream>
@@ -29,10 +30,12 @@ int ceil_log2(size_t n) {
   return lg;
 }
 
+int size_class(size_t n) { return n <= 1 ? 0 : (int)std::lround(std::log2((double)n)); }
+
 MsmConfig msm_config_for(const zk_ctx* ctx, bool g2, size_t n, int dist, int fixed_c) {
   const MsmConfig& base = ctx->msm_cfg[g2 ? 1 : 0];
   if (base.c != 0) return base;  // explicit settings win
-  const auto it = ctx->tune.msm.find(std::make_tuple(g2 ? 2 : 1, ceil_log2(n), dist, fixed_c));
+  const auto it = ctx->tune.msm.find(std::make_tuple(g2 ? 2 : 1, size_class(n), dist, fixed_c));
   if (it == ctx->tune.msm.end()) return base;
   MsmConfig r = it->second;
   r.k1 = base.k1;
@@ -40,7 +43,7 @@ MsmConfig msm_config_for(const zk_ctx* ctx, bool g2, size_t n, int dist, int fix
 }
 
 int table_c_for(const zk_ctx* ctx, bool g2, size_t n, int dist) {
-  const auto it = ctx->tune.table_c.find(std::make_tuple(g2 ? 2 : 1, ceil_log2(n), dist));
+  const auto it = ctx->tune.table_c.find(std::make_tuple(g2 ? 2 : 1, size_class(n), dist));
   return it != ctx->tune.table_c.end() ? it->second : msm_fixed_default_c(n, g2);
 }
 

@@ -8,7 +8,9 @@
 //   * fixed-base MSMs: table window bits (under a memory cap), k0 and chunk;
 //   * NTT: the largest radix of one shared-memory pass (2^bits).
 // A context holds the table; settings given with zk_msm_set_config (c != 0)
-// take precedence over it.  Sizes are keyed by ceil(log2 n).
+// take precedence over it.  Sizes are keyed by round(log2 n), so a circuit
+// of 2^k constraints (a few more witness variables than 2^k) and its H
+// (2^k points) share the entries tuned at 2^k.
 #pragma once
 #include <cstddef>
 #include <cstdint>
@@ -34,6 +36,7 @@ struct TuneTable {
 };
 
 int ceil_log2(size_t n);
+int size_class(size_t n);  // round(log2 n)
 
 // Settings for an MSM of n points: explicit context settings, else the tuned
 // entry, else the defaults.
