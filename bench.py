@@ -63,6 +63,7 @@ def parse_args():
     p.add_argument("--workdir", default=os.environ.get("ZK_BENCH_DIR", "/tmp/zyklop_bench"))
     p.add_argument("--batch-proofs", type=int, default=64, help="0 skips the batched section")
     p.add_argument("--batch-inflight", type=int, default=8)
+    p.add_argument("--batch-group", type=int, default=16)
     p.add_argument("--no-autotune", action="store_true",
                    help="skip the autotuner (default settings for every size)")
     p.add_argument("--serve-seconds", type=float, default=60.0, help="0 skips serving")
@@ -471,14 +472,25 @@ def run_batched(args, dist, ctx, L):
 
     plain_once()  # warm-up: workspaces sized, tables resident
     (lat, plain_proofs), plain_ms = timed(plain_once)
-    api.set_graphs(True, ctx=ctx)
     run = lambda: api.prove_batch([circuits[j] for j in jobs], [wits[j] for j in jobs],
                                   inflight=args.batch_inflight, ctx=ctx)
+    modes = {}
+    # in-flight pipelines with CUDA-graph replay
+    api.set_batch_mode(api.BATCH_INFLIGHT, ctx=ctx)
+    api.set_graphs(True, ctx=ctx)
     run()  # warm-up: graph capture per (workspace, circuit)
-    batched_proofs, batch_ms = timed(run)
+    proofs_inflight, modes["inflight"] = timed(run)
     api.set_graphs(False, ctx=ctx)
-    assert all(np.array_equal(a, b) for a, b in zip(plain_proofs, batched_proofs)), \
-        "batched proofs differ from one-at-a-time proofs"
+    # fused groups (multi-instance MSM chains)
+    api.set_batch_mode(api.BATCH_FUSED, args.batch_group, ctx=ctx)
+    run()  # warm-up: both group workspaces sized
+    proofs_fused, modes["fused"] = timed(run)
+    api.set_batch_mode(api.BATCH_AUTO, ctx=ctx)
+    for got in (proofs_inflight, proofs_fused):
+        assert all(np.array_equal(a, b) for a, b in zip(plain_proofs, got)), \
+            "batched proofs differ from one-at-a-time proofs"
+    best = min(modes, key=modes.get)
+    batch_ms = modes[best]
 
     def files_once():
         for j in jobs:
@@ -496,7 +508,10 @@ def run_batched(args, dist, ctx, L):
         "plain_files_proofs_per_s": n / (files_ms / 1e3),
         "speedup_vs_plain_files": files_ms / batch_ms,
         "plain_latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)},
-        "batched_call": f"zk_prove_batch, {args.batch_inflight} proofs in flight, CUDA graphs",
+        "batched_call": f"zk_prove_batch, {best} mode",
+        "batched_modes_proofs_per_s": {
+            f"inflight ({args.batch_inflight} in flight, CUDA graphs)": n / (modes["inflight"] / 1e3),
+            f"fused (groups of {args.batch_group})": n / (modes["fused"] / 1e3)},
         "autotuned": tuned, "autotune_s": round(t_tune, 1),
         "plain_call": "zk_prove one at a time (same resident circuits and tables)",
         "plain_files_call": "zk_groth16_prove_files one at a time (zkey loaded per proof, "
