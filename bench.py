@@ -76,28 +76,39 @@ def parse_args():
 
 # ------------------------------------------------------------ distributed
 class Dist:
-    def __init__(self):
+    """One process per GPU (torchrun env).  NCCL on GPUs; gloo when CUDA is
+    absent (the host-side logic runs and is tested on CPU that way)."""
+
+    def __init__(self, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.cuda = False
         if self.world > 1:
             import datetime
+            import torch
             import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.cuda = torch.cuda.is_available()
+            backend = backend or ("nccl" if self.cuda else "gloo")
+            self.cuda = backend == "nccl"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.pg = dist
 
     def barrier(self):
         if self.pg:
             import torch
-            self.pg.barrier(device_ids=[self.local])
-            torch.cuda.synchronize()
+            if self.cuda:
+                self.pg.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                self.pg.barrier()
 
     def max(self, x):
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([float(x)], device="cuda")
+        t = torch.tensor([float(x)], device="cuda" if self.cuda else "cpu")
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
