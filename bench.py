@@ -71,6 +71,9 @@ def parse_args():
     p.add_argument("--serve-rate", type=float, default=200.0)
     p.add_argument("--serve-logs", default="16,19,21,23")
     p.add_argument("--serve-inflight", type=int, default=4)
+    p.add_argument("--prim-g1", default="18,20,22,24", help="G1 MSM sizes (log2); empty skips")
+    p.add_argument("--prim-g2", default="18,20")
+    p.add_argument("--prim-ntt", default="16,18,20,22,24")
     return p.parse_args()
 
 
@@ -410,6 +413,122 @@ def run_mine(args, dist):
     return line, (z, w), ctx
 
 
+# -------------------------------------------------------------- primitives
+def hbm_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def prim_inputs(group, log_max, seed):
+    """Points k_i * G (device, SoA) and uniform scalars for the sweep."""
+    from zyklop_b200 import api
+    rng = np.random.default_rng(seed)
+    n = 1 << log_max
+    k = rng.integers(0, 2**63, size=(n, 4), dtype=np.uint64)
+    k[:, 3] &= np.uint64((1 << 60) - 1)
+    px, py = api.mul_generator(group, k, keep_on_device=True)
+    s = rng.integers(0, 2**63, size=(n, 4), dtype=np.uint64)
+    s[:, 3] &= np.uint64((1 << 60) - 1)
+    return px, py, api.to_device(s)
+
+
+def time_calls(fn, reps=3):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t)
+    return float(np.median(ts))
+
+
+def run_primitives(args, msm_fns, ntt_fn, imad_peak):
+    """Config-1 sweep: G1 MSM at 2^18..2^24 and G2 MSM at 2^18, 2^20 (uniform
+    scalars, points k_i G), Fr NTT at 2^16..2^24.  msm_fns[g](px, py, sc, n)
+    and ntt_fn(buf, log_n) are the implementation's calls on device buffers."""
+    import torch
+    out = {"g1_msm": {}, "g2_msm": {}, "ntt": {}}
+    peak_hbm, hbm_src = hbm_peak()
+    for g, logs in ((1, [int(x) for x in args.prim_g1.split(",") if x]),
+                    (2, [int(x) for x in args.prim_g2.split(",") if x])):
+        if not logs:
+            continue
+        px, py, sc = prim_inputs(g, max(logs), 40 + g)
+        for lg in logs:
+            n = 1 << lg
+            t = time_calls(lambda: msm_fns[g](px, py, sc, n))
+            per_point = FP_MULTS_PER_POINT["accum_g1" if g == 1 else "accum_g2"]
+            r = {"ms": t * 1e3, "points_per_s": n / t}
+            if imad_peak:
+                r["imad_frac"] = n * per_point * IMAD_PER_FP_MULT / t / 1e12 / imad_peak
+            out[f"g{g}_msm"][f"2^{lg}"] = r
+        del px, py, sc
+        torch.cuda.empty_cache()
+    for lg in [int(x) for x in args.prim_ntt.split(",") if x]:
+        n = 1 << lg
+        buf = torch.randint(0, 2**62, (n, 4), dtype=torch.int64, device="cuda")
+        buf[:, 3] &= (1 << 58) - 1  # canonical Fr, read as Montgomery
+        t = time_calls(lambda: ntt_fn(buf, lg))
+        r = {"ms": t * 1e3, "gb_per_s": 64 * n / t / 1e9, "hbm_frac": 64 * n / t / 1e9 / peak_hbm}
+        if imad_peak:  # one twiddle product per butterfly: (n / 2) log2 n products
+            r["imad_frac"] = (n // 2) * lg * IMAD_PER_FP_MULT / t / 1e12 / imad_peak
+        out["ntt"][f"2^{lg}"] = r
+        del buf
+    out["conventions"] = (f"MSM work {FP_MULTS_PER_POINT['accum_g1']:.0f} (G1) / "
+                          f"{FP_MULTS_PER_POINT['accum_g2']:.0f} (G2) Fp products per point x "
+                          f"{IMAD_PER_FP_MULT:.0f} IMAD-class ops against the measured IMAD "
+                          f"probe; NTT bytes 64 per element against HBM {peak_hbm:.0f} GB/s "
+                          f"({hbm_src}) and (n/2) log2 n products against the IMAD probe; "
+                          "wall time of the API call, inputs resident")
+    return out
+
+
+def mine_primitives(args, ctx, L, imad_peak):
+    from zyklop_b200 import api
+    from zyklop_b200._lib import check
+    res = np.zeros(16, np.uint64)
+    inf = ctypes.c_int()
+
+    def msm(fn):
+        return lambda px, py, sc, n: check(fn(ctx, api.ptr(px), api.ptr(py), api.ptr(sc), n,
+                                              res.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                              ctypes.byref(inf)))
+
+    def ntt(buf, lg):
+        check(L.zk_ntt(ctx, api.ptr(buf), lg, 0))
+
+    out = run_primitives(args, {1: msm(L.zk_msm_g1), 2: msm(L.zk_msm_g2)}, ntt, imad_peak)
+    out["calls"] = "zk_msm_g1 / zk_msm_g2 (windowed, autotuned where tuned), zk_ntt (forward)"
+    return out
+
+
+def cpu_msm_baseline(lg=18):
+    """The oracle's G1 MSM (C, OpenMP, all host threads) on 2^lg points k_i G
+    (made on the GPU) with uniform scalars."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle
+    from zyklop_b200 import api
+    orc = _oracle.load()
+    rng = np.random.default_rng(7)
+    n = 1 << lg
+    k = rng.integers(0, 2**63, size=(n, 4), dtype=np.uint64)
+    k[:, 3] &= np.uint64((1 << 60) - 1)
+    px, py = api.mul_generator(1, k)
+    s = rng.integers(0, 2**63, size=(n, 4), dtype=np.uint64)
+    s[:, 3] &= np.uint64((1 << 60) - 1)
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    orc.msm_g1(px, py, s, threads=threads)
+    t = time.perf_counter() - t
+    return {"value": n / t, "unit": "points/s", "cores": threads, "kind": "port",
+            "sample": f"one 2^{lg}-point G1 MSM by the CPU oracle (C, OpenMP; {t:.2f} s)"}
+
+
 # -------------------------------------------------------------- autotuning
 def autotune_sizes(args, api, ctx, logs, witness_dist, max_table_bytes=16 << 30, table_upto=21):
     """Fixed-base table window bits and MSM settings for circuits of 2^lg
@@ -665,6 +784,7 @@ def run_reference(args, dist):
     ms = dist.max(start.elapsed_time(end))
     value = args.gpus * args.steps / (ms / 1e3)
     n_vars = int.from_bytes(open(w, "rb").read()[60:64], "little")
+    prims = reference_primitives(args)
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -678,7 +798,41 @@ def run_reference(args, dist):
                                    "every step a full proof"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "clocks": clk,
+        "primitives": prims,
     }
+
+
+def reference_primitives(args):
+    """The same config-1 sweep through the reference build's own primitives
+    (msm_g1, msm_g2_device, ntt) on device buffers."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libzkref_prims.so")
+    if not os.path.exists(path) or not (args.prim_g1 or args.prim_g2 or args.prim_ntt):
+        return None
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    L = ctypes.CDLL(path)
+    for name in ("zkref_msm_g1_device", "zkref_msm_g2_device"):
+        fn = getattr(L, name)
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, u64p]
+        fn.restype = ctypes.c_int
+    L.zkref_ntt_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.zkref_ntt_device.restype = ctypes.c_int
+    out = np.zeros(16, np.uint64)
+
+    def msm(fn):
+        def call(px, py, sc, n):
+            with silenced():
+                fn(ctypes.c_void_p(px.data_ptr()), ctypes.c_void_p(py.data_ptr()),
+                   ctypes.c_void_p(sc.data_ptr()), n, out.ctypes.data_as(u64p))
+        return call
+
+    def ntt(buf, lg):
+        with silenced():
+            L.zkref_ntt_device(ctypes.c_void_p(buf.data_ptr()), lg, 0)
+
+    r = run_primitives(args, {1: msm(L.zkref_msm_g1_device), 2: msm(L.zkref_msm_g2_device)},
+                       ntt, None)
+    r["calls"] = "the reference's msm_g1, msm_g2_device and ntt (oracle/_ref/libzkref_prims.so)"
+    return r
 
 
 def lib_handle():
@@ -705,6 +859,13 @@ def main():
             line["batched"] = run_batched(args, dist, ctx, lib_handle())
         if dist.world == 1 and args.serve_seconds > 0:
             line["serving"] = run_serving(args, dist, ctx, lib_handle())
+        if dist.world == 1 and (args.prim_g1 or args.prim_g2 or args.prim_ntt):
+            line["primitives"] = mine_primitives(args, ctx, lib_handle(),
+                                                 line["roofline"]["peak"])
+            if not args.no_cpu_baseline:
+                cb = cpu_msm_baseline()
+                if cb:
+                    line["primitives"]["cpu_baseline_g1_msm"] = cb
         lib_handle().zk_ctx_destroy(ctx)
         if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(*files)
