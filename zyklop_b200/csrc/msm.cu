@@ -555,6 +555,14 @@ __global__ void __launch_bounds__(kRedT) k_msm_reduce_blk(
 // section, for w < W = 254 / c + 1.  With these, all windows of a fixed-base
 // MSM share one bucket set: one bucket reduction instead of W, and no
 // doubling chain between windows.
+//
+// The affine conversions share inversions (Montgomery's trick): a thread
+// doubles through kPreChunk windows, writing each multiple's X, Y into its
+// table record and keeping ZZ, ZZZ and the running product of the ZZZs, then
+// inverts that product once and walks back, so a chunk costs one inversion
+// and ~7 products per record instead of one inversion per record.
+constexpr int kPreChunk = 8;
+
 template <class F>
 __global__ void __launch_bounds__(128) k_msm_precompute(const F* __restrict__ px,
                                                         const F* __restrict__ py, uint32_t pstride,
@@ -565,18 +573,38 @@ __global__ void __launch_bounds__(128) k_msm_precompute(const F* __restrict__ px
   const F x = ld_pod(px + i * pstride), y = ld_pod(py + i * pstride);
   st_pod(table + 2 * i, x);
   st_pod(table + 2 * i + 1, y);
-  xyzz<F> acc;
   const bool inf = fe_is_zero(x) && fe_is_zero(y);
+  xyzz<F> acc;
   if (!inf) acc = xyzz<F>{x, y, fe_one_of<F>(), fe_one_of<F>()};
-  for (int w = 1; w < W; w++) {
-    affine<F> a{fe_zero_of<F>(), fe_zero_of<F>()};
-    if (!inf) {
-      for (int d = 0; d < c; d++) acc = xyzz_dbl(acc);
-      a = xyzz_to_affine(acc);
+  for (int w0 = 1; w0 < W; w0 += kPreChunk) {
+    const int cnt = min(kPreChunk, W - w0);
+    F zz[kPreChunk], zzz[kPreChunk], pre[kPreChunk];
+    F prod = fe_one_of<F>();
+    for (int k = 0; k < cnt; k++) {
+      const size_t rec = (size_t)(w0 + k) * n + i;
+      if (!inf)
+        for (int d = 0; d < c; d++) acc = xyzz_dbl(acc);
+      // a multiple at infinity (only for points outside the order-r
+      // subgroup) takes 1 in the product and is written as (0, 0)
+      const bool at_inf = inf || xyzz_is_inf(acc);
+      zz[k] = at_inf ? fe_zero_of<F>() : acc.zz;
+      zzz[k] = at_inf ? fe_one_of<F>() : acc.zzz;
+      prod = prod * zzz[k];
+      pre[k] = prod;
+      st_pod(table + 2 * rec, at_inf ? fe_zero_of<F>() : acc.x);
+      st_pod(table + 2 * rec + 1, at_inf ? fe_zero_of<F>() : acc.y);
     }
-    const size_t rec = (size_t)w * n + i;
-    st_pod(table + 2 * rec, a.x);
-    st_pod(table + 2 * rec + 1, a.y);
+    F inv = fe_inv(prod);  // 1 / (zzz_0 ... zzz_{cnt-1})
+    for (int k = cnt - 1; k >= 0; k--) {
+      const F zzzi = k ? inv * pre[k - 1] : inv;  // 1 / zzz_k
+      inv = inv * zzz[k];
+      if (fe_is_zero(zz[k])) continue;  // stored as (0, 0) already
+      const size_t rec = (size_t)(w0 + k) * n + i;
+      const F zi = zzzi * zz[k];  // ZZ / ZZZ = 1 / Z
+      const F zzi = fe_sqr(zi);   // 1 / ZZ
+      st_pod(table + 2 * rec, ld_pod(table + 2 * rec) * zzi);
+      st_pod(table + 2 * rec + 1, ld_pod(table + 2 * rec + 1) * zzzi);
+    }
   }
 }
 
