@@ -233,8 +233,40 @@ def test_malformed_inputs_are_status_codes(api, files, tmp_path):
     with pytest.raises(ZkError) as e:
         c.prove(api.read_wtns(w)[:10])
     assert e.value.code == 6  # ZK_EWITNESS
+    # a section-4 entry naming a signal beyond nVars: rejected by the
+    # resident load and by the one-shot call (which checks it after proving)
+    bad = bytearray(data)
+    off = section_offset(data, 4)
+    bad[off + 4 + 8:off + 4 + 12] = (0xFFFFFFF0).to_bytes(4, "little")  # entry 0, signal
+    (tmp_path / "sig.zkey").write_bytes(bytes(bad))
+    with pytest.raises(ZkError) as e:
+        api.Circuit(tmp_path / "sig.zkey")
+    assert e.value.code == 5
+    with pytest.raises(ZkError) as e:
+        api.prove_files(tmp_path / "sig.zkey", w)
+    assert e.value.code == 5
+    # a witness with fewer values than the circuit's nVars, one-shot
+    wb = bytearray(blob(w))
+    o1 = section_offset(bytes(wb), 1)
+    wb[o1 + 36:o1 + 40] = (10).to_bytes(4, "little")
+    (tmp_path / "short.wtns").write_bytes(bytes(wb))
+    with pytest.raises(ZkError) as e:
+        api.prove_files(z, tmp_path / "short.wtns")
+    assert e.value.code == 6
     # the context stays usable after the failures
     assert np.array_equal(c.prove(api.read_wtns(w)), api.prove_files(z, w))
+
+
+def section_offset(data, kind):
+    """Byte offset of the first section of `kind` in a snarkjs BinFile."""
+    pos = 12
+    for _ in range(int.from_bytes(data[8:12], "little")):
+        t = int.from_bytes(data[pos:pos + 4], "little")
+        size = int.from_bytes(data[pos + 4:pos + 12], "little")
+        if t == kind:
+            return pos + 12
+        pos += 12 + size
+    raise KeyError(kind)
 
 
 @pytest.mark.parametrize("graphs", [False, True])

@@ -224,8 +224,7 @@ int zk_groth16_prove_mem(zk_ctx* ctx, const uint8_t* zkey, size_t zkey_len, cons
   auto zf = BinFile::wrap(zkey, zkey_len, "zkey", 1);
   auto wf = BinFile::wrap(wtns, wtns_len, "wtns", 2);
   const WtnsView w = parse_wtns(*wf);
-  std::unique_ptr<zk_circuit> c(circuit_load(ctx, *zf));
-  prove(c.get(), w.values, w.n_vars, false, nullptr, nullptr, proof, nullptr);
+  prove_oneshot(ctx, *zf, w.values, w.n_vars, proof);
   ZK_API_END
 }
 
@@ -238,8 +237,7 @@ int zk_groth16_prove_files(zk_ctx* ctx, const char* zkey_path, const char* wtns_
   auto zf = BinFile::open(zkey_path, "zkey", 1);
   auto wf = BinFile::open(wtns_path, "wtns", 2);
   const WtnsView w = parse_wtns(*wf);
-  std::unique_ptr<zk_circuit> c(circuit_load(ctx, *zf));
-  prove(c.get(), w.values, w.n_vars, false, nullptr, nullptr, proof, nullptr);
+  prove_oneshot(ctx, *zf, w.values, w.n_vars, proof);
   ZK_API_END
 }
 

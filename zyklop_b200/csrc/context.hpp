@@ -31,6 +31,7 @@ struct ProveWs {
   DeviceBuffer we, aw, bw, cw, h;
   DeviceBuffer msm[kStreams];
   PinnedBuffer win[kStreams];
+  PinnedBuffer flag;  // small host-visible status words (section-4 check)
   MsmResult res[kStreams];
   MsmConfig cfg[kStreams];  // settings of each MSM of the current proof
   // captured pipelines, one per (circuit, blinding); all are dropped when a

@@ -140,8 +140,10 @@ ProveWs::~ProveWs() {
   drop_graph();
 }
 
-zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
-  const ZkeyView z = parse_zkey(f);
+namespace {
+
+// Sizes and verification-key points of a parsed zkey (no device work).
+std::unique_ptr<zk_circuit> circuit_header(zk_ctx* ctx, const ZkeyView& z) {
   std::unique_ptr<zk_circuit> c(new zk_circuit());
   c->ctx = ctx;
   c->id = next_circuit_id();
@@ -158,32 +160,57 @@ zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
   memcpy(c->delta1, z.delta1, 64);
   memcpy(c->delta2, z.delta2, 128);
   if (z.ic) c->ic.assign(z.ic, z.ic + 8 * ((size_t)c->l + 1));
-  cudaStream_t st = ctx->stream;
-  Stager& sg = ctx->stager;
-  const size_t m1 = c->m1, nc = (size_t)c->m1 - c->l - 1;
-  // CRS points: record 0 of A / B1 / B2 is alpha1 / beta1 / beta2
-  c->pts_a.ensure(64 * (m1 + 1));
-  ZK_CUDA(cudaMemcpyAsync(c->pts_a.ptr, c->alpha1, 64, cudaMemcpyHostToDevice, st));
-  sg.upload(c->pts_a.as<char>() + 64, z.a, 64 * m1, st);
-  c->pts_b2.ensure(128 * (m1 + 1));
-  ZK_CUDA(cudaMemcpyAsync(c->pts_b2.ptr, c->beta2, 128, cudaMemcpyHostToDevice, st));
-  sg.upload(c->pts_b2.as<char>() + 128, z.b2, 128 * m1, st);
-  if (z.b1) {
-    c->has_b1 = true;
-    c->pts_b1.ensure(64 * (m1 + 1));
-    ZK_CUDA(cudaMemcpyAsync(c->pts_b1.ptr, c->beta1, 64, cudaMemcpyHostToDevice, st));
-    sg.upload(c->pts_b1.as<char>() + 64, z.b1, 64 * m1, st);
-  }
-  c->pts_c.ensure(64 * (nc ? nc : 1));
-  sg.upload(c->pts_c.ptr, z.c, 64 * nc, st);
-  c->pts_h.ensure(64 * (size_t)c->n);
-  sg.upload(c->pts_h.ptr, z.h, 64 * (size_t)c->n, st);
+  c->has_b1 = z.b1 != nullptr;
+  return c;
+}
 
-  // section 4 -> CSR on the device
-  const size_t nnz = c->n_coefs, n = c->n;
+enum PointSet { kSetA, kSetB1, kSetB2, kSetC, kSetH };
+
+// Uploads one CRS point set on `st` (record 0 of A / B1 / B2 is alpha1 /
+// beta1 / beta2, like the reference's extended buffers,
+// src/groth16.cu:1199-1227).  Returns once the host source may be released;
+// the copy completes in stream order.
+void upload_points(zk_circuit* c, const ZkeyView& z, PointSet set, cudaStream_t st, Stager& sg) {
+  const size_t m1 = c->m1, nc = m1 - c->l - 1;
+  switch (set) {
+    case kSetA:
+      c->pts_a.ensure(64 * (m1 + 1));
+      ZK_CUDA(cudaMemcpyAsync(c->pts_a.ptr, c->alpha1, 64, cudaMemcpyHostToDevice, st));
+      sg.upload(c->pts_a.as<char>() + 64, z.a, 64 * m1, st);
+      break;
+    case kSetB1:
+      if (!z.b1) return;
+      c->pts_b1.ensure(64 * (m1 + 1));
+      ZK_CUDA(cudaMemcpyAsync(c->pts_b1.ptr, c->beta1, 64, cudaMemcpyHostToDevice, st));
+      sg.upload(c->pts_b1.as<char>() + 64, z.b1, 64 * m1, st);
+      break;
+    case kSetB2:
+      c->pts_b2.ensure(128 * (m1 + 1));
+      ZK_CUDA(cudaMemcpyAsync(c->pts_b2.ptr, c->beta2, 128, cudaMemcpyHostToDevice, st));
+      sg.upload(c->pts_b2.as<char>() + 128, z.b2, 128 * m1, st);
+      break;
+    case kSetC:
+      c->pts_c.ensure(64 * (nc ? nc : 1));
+      sg.upload(c->pts_c.ptr, z.c, 64 * nc, st);
+      break;
+    case kSetH:
+      c->pts_h.ensure(64 * (size_t)c->n);
+      sg.upload(c->pts_h.ptr, z.h, 64 * (size_t)c->n, st);
+      break;
+  }
+}
+
+// Section 4 -> CSR on the device (the reference builds it on the host,
+// src/groth16.cu:737-809).  Enqueued on `st`; *h_bad receives the count of
+// entries outside the domain or witness once `st` reaches the copy.
+struct CsrScratch {
   DeviceBuffer raw, tmp;
-  raw.ensure(44 * (nnz ? nnz : 1));
-  sg.upload(raw.ptr, z.coefs, 44 * nnz, st);
+};
+void build_csr(zk_circuit* c, const ZkeyView& z, cudaStream_t st, Stager& sg, CsrScratch& s,
+               uint32_t* h_bad) {
+  const size_t nnz = c->n_coefs, n = c->n;
+  s.raw.ensure(44 * (nnz ? nnz : 1));
+  sg.upload(s.raw.ptr, z.coefs, 44 * nnz, st);
   const size_t tiles = scan::tile_count(n + 1) + 1;
   auto carve_csr_tmp = [&](void* base, uint32_t** cnt, uint32_t** cur, uint32_t** tl,
                            uint32_t** bad) {
@@ -195,31 +222,43 @@ zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
     return cv.off;
   };
   uint32_t *cnt[2], *cur[2], *tl[2], *bad;
-  tmp.ensure(carve_csr_tmp(nullptr, cnt, cur, tl, &bad));  // dry run: size with padding
-  carve_csr_tmp(tmp.ptr, cnt, cur, tl, &bad);
-  ZK_CUDA(cudaMemsetAsync(tmp.ptr, 0, tmp.cap, st));
+  s.tmp.ensure(carve_csr_tmp(nullptr, cnt, cur, tl, &bad));  // dry run: size with padding
+  carve_csr_tmp(s.tmp.ptr, cnt, cur, tl, &bad);
+  ZK_CUDA(cudaMemsetAsync(s.tmp.ptr, 0, s.tmp.cap, st));
   for (int m = 0; m < 2; m++) {
     c->row[m].ensure(4 * (n + 1));
     c->sig[m].ensure(4 * (nnz ? nnz : 1));
     c->val[m].ensure(32 * (nnz ? nnz : 1));
   }
   if (nnz) {
-    k_coef_count<<<blocks(nnz, 256), 256, 0, st>>>(raw.as<uint32_t>(), (uint32_t)nnz, (uint32_t)n,
+    k_coef_count<<<blocks(nnz, 256), 256, 0, st>>>(s.raw.as<uint32_t>(), (uint32_t)nnz, (uint32_t)n,
                                                   c->m1, cnt[0], cnt[1], bad);
     ZK_LAUNCHED();
   }
   for (int m = 0; m < 2; m++) scan::exclusive(cnt[m], cur[m], n + 1, tl[m], st);
   if (nnz) {
     k_coef_scatter<<<blocks(nnz, 256), 256, 0, st>>>(
-        raw.as<uint32_t>(), (uint32_t)nnz, (uint32_t)n, c->m1, cur[0], cur[1],
+        s.raw.as<uint32_t>(), (uint32_t)nnz, (uint32_t)n, c->m1, cur[0], cur[1],
         c->sig[0].as<uint32_t>(), c->sig[1].as<uint32_t>(), c->val[0].as<uint32_t>(),
         c->val[1].as<uint32_t>());
     ZK_LAUNCHED();
   }
   for (int m = 0; m < 2; m++)
     ZK_CUDA(cudaMemcpyAsync(c->row[m].ptr, cnt[m], 4 * (n + 1), cudaMemcpyDeviceToDevice, st));
+  ZK_CUDA(cudaMemcpyAsync(h_bad, bad, 4, cudaMemcpyDeviceToHost, st));
+}
+
+}  // namespace
+
+zk_circuit* circuit_load(zk_ctx* ctx, const BinFile& f) {
+  const ZkeyView z = parse_zkey(f);
+  std::unique_ptr<zk_circuit> c = circuit_header(ctx, z);
+  cudaStream_t st = ctx->stream;
+  Stager& sg = ctx->stager;
+  for (PointSet set : {kSetA, kSetB2, kSetB1, kSetC, kSetH}) upload_points(c.get(), z, set, st, sg);
+  CsrScratch scratch;
   uint32_t h_bad = 0;
-  ZK_CUDA(cudaMemcpyAsync(&h_bad, bad, 4, cudaMemcpyDeviceToHost, st));
+  build_csr(c.get(), z, st, sg, scratch, &h_bad);
   ZK_CUDA(cudaStreamSynchronize(st));
   ZK_REQUIRE(h_bad == 0, ZK_EFORMAT, "zkey: section 4 has entries outside the domain or witness");
   ctx->ntt.ensure(c->log_n, st);
@@ -335,6 +374,30 @@ void ws_stage(zk_circuit* c, ProveWs& ws, const uint64_t* witness, bool on_devic
     stager.upload(we + 4, witness, 32 * (size_t)c->m1, s0);
 }
 
+// MSM i of a proof (indexed like ProveWs::msm) on stream i mod nstreams,
+// after the staged witness; its window sums land in ws.win[i] and
+// ev_done[i] marks them.
+void ws_msm(zk_circuit* c, ProveWs& ws, int i, bool g2, const DeviceBuffer& pts,
+            const DeviceBuffer& tab, const uint64_t* sc, size_t cnt) {
+  const bool fixed = c->tab_c[0] != 0;
+  const int si = i % ws.nstreams;
+  cudaStream_t st = ws.st[si];
+  if (si) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
+  if (fixed)
+    ws.res[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
+                                  ws.msm[i].cap, ws.cfg[i], st);
+  else if (g2)
+    ws.res[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap,
+                               ws.cfg[i], st);
+  else
+    ws.res[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap,
+                               ws.cfg[i], st);
+  ZK_REQUIRE(ws.res[i].bytes <= kMaxWindowBytes, ZK_EINTERNAL, "prove: MSM result too large");
+  ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, ws.res[i].d_data, ws.res[i].bytes, cudaMemcpyDeviceToHost,
+                          st));
+  ZK_CUDA(cudaEventRecord(ws.ev_done[i], st));
+}
+
 // The device part of a proof, from the staged witness to the MSM results in
 // pinned host memory.  It begins and ends on stream 0 (other streams fork
 // from and join back to it), issues no synchronizing call, and can therefore
@@ -342,29 +405,11 @@ void ws_stage(zk_circuit* c, ProveWs& ws, const uint64_t* witness, bool on_devic
 void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg) {
   zk_ctx* ctx = c->ctx;
   const size_t m1 = c->m1, n = c->n, l = c->l, nc = m1 - l - 1;
-  const bool fixed = c->tab_c[0] != 0;
   cudaStream_t s0 = ws.st[0];
   uint64_t* we = ws.we.as<uint64_t>();
   ZK_CUDA(cudaEventRecord(ws.ev_we, s0));
   auto launch = [&](int i, bool g2, const DeviceBuffer& pts, const DeviceBuffer& tab,
-                    const uint64_t* sc, size_t cnt) {
-    const int si = i % ws.nstreams;
-    cudaStream_t st = ws.st[si];
-    if (si) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
-    if (fixed)
-      ws.res[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
-                                    ws.msm[i].cap, ws.cfg[i], st);
-    else if (g2)
-      ws.res[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr,
-                                 ws.msm[i].cap, ws.cfg[i], st);
-    else
-      ws.res[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr,
-                                 ws.msm[i].cap, ws.cfg[i], st);
-    ZK_REQUIRE(ws.res[i].bytes <= kMaxWindowBytes, ZK_EINTERNAL, "prove: MSM result too large");
-    ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, ws.res[i].d_data, ws.res[i].bytes,
-                            cudaMemcpyDeviceToHost, st));
-    ZK_CUDA(cudaEventRecord(ws.ev_done[i], st));
-  };
+                    const uint64_t* sc, size_t cnt) { ws_msm(c, ws, i, g2, pts, tab, sc, cnt); };
   launch(1, false, c->pts_a, c->tab_a, we, m1 + 1);
   launch(2, true, c->pts_b2, c->tab_b2, we, m1 + 1);
   launch(3, false, c->pts_c, c->tab_c_pts, we + 4 * (l + 2), nc);
@@ -565,6 +610,52 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   ZK_CUDA(cudaEventRecord(ws.ev_all, ws.st[0]));
   ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_all, 0));
   ws_finish(c, ws, blind, r, s, proof);
+}
+
+void prove_oneshot(zk_ctx* ctx, const BinFile& zkey, const uint64_t* witness, size_t n_witness,
+                   uint64_t proof[32]) {
+  const ZkeyView z = parse_zkey(zkey);
+  std::unique_ptr<zk_circuit> cp = circuit_header(ctx, z);
+  zk_circuit* c = cp.get();
+  check_job(c, witness, n_witness, false);
+  note_witness(c, witness, false);
+  ProveWs& ws = ctx->ws;
+  ws_prepare(c, ws, false);
+  ws.flag.ensure(256);
+  Stager& sg = ctx->stager;
+  const size_t m1 = c->m1, n = c->n, l = c->l, nc = m1 - l - 1;
+  cudaStream_t s0 = ws.st[0];
+  ZK_CUDA(cudaEventRecord(ws.ev_begin, ctx->stream));
+  for (int i = 0; i < ProveWs::kStreams; i++) ZK_CUDA(cudaStreamWaitEvent(ws.st[i], ws.ev_begin, 0));
+  ws_stage(c, ws, witness, false, sg);
+  ZK_CUDA(cudaEventRecord(ws.ev_we, s0));
+  const uint64_t* we = ws.we.as<uint64_t>();
+  const DeviceBuffer none;
+  // each point set goes up on the stream of the MSM that reads it, and that
+  // MSM starts at once; B2 (the longest MSM) first
+  upload_points(c, z, kSetB2, ws.st[2 % ws.nstreams], sg);
+  ws_msm(c, ws, 2, true, c->pts_b2, none, we, m1 + 1);
+  upload_points(c, z, kSetA, ws.st[1 % ws.nstreams], sg);
+  ws_msm(c, ws, 1, false, c->pts_a, none, we, m1 + 1);
+  upload_points(c, z, kSetC, ws.st[3 % ws.nstreams], sg);
+  ws_msm(c, ws, 3, false, c->pts_c, none, we + 4 * (l + 2), nc);
+  // section 4 -> CSR -> A.w, B.w -> h on stream 0, the H points beside it
+  CsrScratch csr;
+  uint32_t* h_bad = ws.flag.as<uint32_t>();
+  build_csr(c, z, s0, sg, csr, h_bad);
+  spmv_enqueue(c, we, ws.aw.as<uint64_t>(), ws.bw.as<uint64_t>(), s0);
+  hpoly(ctx->ntt, ws.aw.as<uint64_t>(), ws.bw.as<uint64_t>(), ws.cw.as<uint64_t>(), c->log_n,
+        ws.h.as<uint64_t>(), s0);
+  cudaStream_t sh = ws.st[4];
+  upload_points(c, z, kSetH, sh, sg);
+  ZK_CUDA(cudaEventRecord(ws.ev_done[4], sh));
+  ZK_CUDA(cudaStreamWaitEvent(s0, ws.ev_done[4], 0));
+  ws_msm(c, ws, 0, false, c->pts_h, none, ws.h.as<uint64_t>(), n);
+  for (int i = 1; i < 4; i++) ZK_CUDA(cudaStreamWaitEvent(s0, ws.ev_done[i], 0));
+  ZK_CUDA(cudaEventRecord(ws.ev_all, s0));
+  ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_all, 0));
+  ws_finish(c, ws, false, nullptr, nullptr, proof);
+  ZK_REQUIRE(*h_bad == 0, ZK_EFORMAT, "zkey: section 4 has entries outside the domain or witness");
 }
 
 void prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* cs, const uint64_t* const* wits,

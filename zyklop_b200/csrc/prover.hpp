@@ -77,6 +77,14 @@ int msm_fixed_default_c(size_t n, bool g2);
 void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool witness_on_device,
            const uint64_t* r, const uint64_t* s, uint64_t proof[32], ProveIntermediates* dbg);
 
+// One-shot unblinded proof from a parsed zkey and a host witness, without a
+// resident circuit: each CRS point set is uploaded on the stream of the MSM
+// that reads it and that MSM starts at once, so the upload of the rest
+// overlaps the MSMs already running; B1 (used only for blinding) is not
+// uploaded.  The same result as circuit_load + prove.
+void prove_oneshot(zk_ctx* ctx, const BinFile& zkey, const uint64_t* witness, size_t n_witness,
+                   uint64_t proof[32]);
+
 // Proves `count` jobs (circuits of one context, witnesses host or device)
 // with up to `inflight` proofs on the GPU at once, each on its own workspace
 // and streams; the host combination of one proof overlaps the GPU work of the
