@@ -242,8 +242,8 @@ int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk) 
   std::lock_guard<std::mutex> g(ctx->mu);
   ZK_REQUIRE(group == 1 || group == 2, ZK_EINVAL, "zk_msm_set_config: group must be 1 or 2");
   ZK_REQUIRE(c == 0 || (c >= 4 && c <= 21), ZK_EINVAL, "zk_msm_set_config: c must be 0 or 4..21");
-  ZK_REQUIRE(k0 >= 1 && k0 <= 4096 && k1 >= 2 && k1 <= 4096, ZK_EINVAL,
-             "zk_msm_set_config: k0 in 1..4096, k1 in 2..4096");
+  ZK_REQUIRE(k0 >= 0 && k0 <= 4096 && k1 >= 2 && k1 <= 4096, ZK_EINVAL,
+             "zk_msm_set_config: k0 in 0..4096 (0 = by size), k1 in 2..4096");
   ZK_REQUIRE(chunk >= 2 && chunk <= 4096 && (chunk & (chunk - 1)) == 0, ZK_EINVAL,
              "zk_msm_set_config: chunk must be a power of two in 2..4096");
   MsmConfig& m = ctx->msm_cfg[group - 1];

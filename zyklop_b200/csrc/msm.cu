@@ -53,7 +53,7 @@ Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false, in
   s.B = 1u << (s.c - 1);
   s.entries = (size_t)s.Wk * s.B + 1;
   s.records = std::max<size_t>((size_t)s.W * n, 1);
-  s.k0 = cfg.k0;
+  s.k0 = cfg.k0 > 0 ? cfg.k0 : msm_default_k0(n, fixed);
   s.k1 = cfg.k1;
   s.chunk = cfg.chunk;
   s.J = (s.B + s.chunk - 1) / s.chunk;
@@ -700,14 +700,26 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
 
 }  // namespace
 
+// Defaults from autotuner runs on uniform scalars (G1 and G2 agree within a
+// few percent): window bits lg - 4 up to 2^16 points, then lg - 3 capped at
+// 16 through 2^22 (a window's 2^15 buckets of XYZZ sums stay L2-resident),
+// growing again by one per doubling beyond 2^22; records per accumulation
+// thread 64 below 2^18 points, 128 below 2^22, 256 beyond.
 int msm_default_c(size_t n, bool g2) {
-  // ~N / 2^c records per bucket; tuned by measurement (see bench sweeps)
+  (void)g2;
   int lg = 0;
   while ((size_t(1) << lg) < n) lg++;
-  int c = lg - (g2 ? 4 : 4);
+  int c = lg <= 16 ? lg - 4 : std::min(lg - 3, 16 + std::max(0, lg - 22));
   if (c < 4) c = 4;
-  if (c > 18) c = 18;
+  if (c > 20) c = 20;
   return c;
+}
+
+int msm_default_k0(size_t n, bool fixed) {
+  if (fixed) return 64;
+  int lg = 0;
+  while ((size_t(1) << lg) < n) lg++;
+  return lg < 18 ? 64 : (lg < 22 ? 128 : 256);
 }
 
 size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg) {

@@ -34,7 +34,8 @@ namespace zk {
 
 struct MsmConfig {
   int c = 0;          // window bits (0 = choose from n)
-  int k0 = 64;        // sorted records per thread in the first accumulation level
+  int k0 = 0;         // sorted records per thread in the first accumulation level
+                      // (0 = choose from n)
   int k1 = 16;        // partial records per thread in later levels
   int chunk = 16;     // buckets per thread in the bucket reduction
   bool operator==(const MsmConfig& o) const {
@@ -67,6 +68,7 @@ struct MsmResult {
 };
 
 int msm_default_c(size_t n, bool g2);
+int msm_default_k0(size_t n, bool fixed);
 
 // Device scratch bytes one MSM of n points needs with this configuration.
 size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg);
