@@ -86,7 +86,7 @@ def msm_g2(px, py, scalars, ctx=None):
     return _msm(lib().zk_msm_g2, 16, px, py, scalars, ctx)
 
 
-def msm_set_config(group, c=0, k0=0, k1=16, chunk=16, ctx=None):
+def msm_set_config(group, c=0, k0=0, k1=16, chunk=0, ctx=None):
     check(lib().zk_msm_set_config(ctx, group, c, k0, k1, chunk))
 
 

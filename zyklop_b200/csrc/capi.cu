@@ -244,8 +244,8 @@ int zk_msm_set_config(zk_ctx* ctx, int group, int c, int k0, int k1, int chunk) 
   ZK_REQUIRE(c == 0 || (c >= 4 && c <= 21), ZK_EINVAL, "zk_msm_set_config: c must be 0 or 4..21");
   ZK_REQUIRE(k0 >= 0 && k0 <= 4096 && k1 >= 2 && k1 <= 4096, ZK_EINVAL,
              "zk_msm_set_config: k0 in 0..4096 (0 = by size), k1 in 2..4096");
-  ZK_REQUIRE(chunk >= 2 && chunk <= 4096 && (chunk & (chunk - 1)) == 0, ZK_EINVAL,
-             "zk_msm_set_config: chunk must be a power of two in 2..4096");
+  ZK_REQUIRE(chunk == 0 || (chunk >= 2 && chunk <= 4096 && (chunk & (chunk - 1)) == 0), ZK_EINVAL,
+             "zk_msm_set_config: chunk must be 0 (by size) or a power of two in 2..4096");
   MsmConfig& m = ctx->msm_cfg[group - 1];
   m.c = c;
   m.k0 = k0;

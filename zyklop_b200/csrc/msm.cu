@@ -55,7 +55,7 @@ Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false, in
   s.records = std::max<size_t>((size_t)s.W * n, 1);
   s.k0 = cfg.k0 > 0 ? cfg.k0 : msm_default_k0(n, fixed);
   s.k1 = cfg.k1;
-  s.chunk = cfg.chunk;
+  s.chunk = cfg.chunk > 0 ? cfg.chunk : msm_default_chunk(n);
   s.J = (s.B + s.chunk - 1) / s.chunk;
   size_t rec = s.records;
   int per_thread = s.k0;
@@ -700,11 +700,14 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
 
 }  // namespace
 
-// Defaults from autotuner runs on uniform scalars (G1 and G2 agree within a
-// few percent): window bits lg - 4 up to 2^16 points, then lg - 3 capped at
-// 16 through 2^22 (a window's 2^15 buckets of XYZZ sums stay L2-resident),
-// growing again by one per doubling beyond 2^22; records per accumulation
-// thread 64 below 2^18 points, 128 below 2^22, 256 beyond.
+// Defaults from autotuner runs (G1 and G2 agree within a few percent):
+// window bits lg - 4 up to 2^16 points, then lg - 3 capped at 16 through
+// 2^22 (a window's 2^15 buckets of XYZZ sums stay L2-resident), growing
+// again by one per doubling beyond 2^22; records per accumulation thread 16
+// up to 2^15 points, 32 up to 2^17, then 64 (fixed-base) or
+// 128 / 256 (windowed, below / from 2^22); buckets per reduction thread 4
+// up to 2^16 points, 8 up to 2^18, then 16.  Small MSMs are bound by the
+// depth of their dependent additions, so they get short per-thread runs.
 int msm_default_c(size_t n, bool g2) {
   (void)g2;
   int lg = 0;
@@ -716,10 +719,18 @@ int msm_default_c(size_t n, bool g2) {
 }
 
 int msm_default_k0(size_t n, bool fixed) {
-  if (fixed) return 64;
   int lg = 0;
   while ((size_t(1) << lg) < n) lg++;
-  return lg < 18 ? 64 : (lg < 22 ? 128 : 256);
+  if (lg <= 15) return 16;
+  if (lg <= 17) return 32;
+  if (fixed) return 64;
+  return lg < 22 ? 128 : 256;
+}
+
+int msm_default_chunk(size_t n) {
+  int lg = 0;
+  while ((size_t(1) << lg) < n) lg++;
+  return lg <= 16 ? 4 : (lg <= 18 ? 8 : 16);
 }
 
 size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg) {

@@ -37,7 +37,7 @@ struct MsmConfig {
   int k0 = 0;         // sorted records per thread in the first accumulation level
                       // (0 = choose from n)
   int k1 = 16;        // partial records per thread in later levels
-  int chunk = 16;     // buckets per thread in the bucket reduction
+  int chunk = 0;      // buckets per thread in the bucket reduction (0 = choose from n)
   bool operator==(const MsmConfig& o) const {
     return c == o.c && k0 == o.k0 && k1 == o.k1 && chunk == o.chunk;
   }
@@ -69,6 +69,7 @@ struct MsmResult {
 
 int msm_default_c(size_t n, bool g2);
 int msm_default_k0(size_t n, bool fixed);
+int msm_default_chunk(size_t n);
 
 // Device scratch bytes one MSM of n points needs with this configuration.
 size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg);

@@ -82,7 +82,10 @@ extern "C" int zk_msm_g1_noalloc(const uint64_t* d_px, const uint64_t* d_py,
   }
   ZK_API_BEGIN
   zk::set_current_profiler(nullptr);  // no event recording (it would create events)
-  const zk::MsmConfig cfg;
+  // fixed settings: the 24 MiB bound above is checked against this layout
+  zk::MsmConfig cfg;
+  cfg.k0 = 64;
+  cfg.chunk = 16;
   ZK_REQUIRE(zk::msm_scratch_bytes(n, false, cfg) <= kNoAllocScratchBytes, ZK_EINTERNAL,
              "zk_msm_g1_noalloc: scratch layout exceeds the fixed array");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
