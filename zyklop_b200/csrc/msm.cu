@@ -35,6 +35,7 @@ struct Shape {
   int levels;            // segmented-reduction levels (>= 1)
   size_t lvl_records[24];
   size_t lvl_blocks[24];
+  int lvl_k[24];         // records per thread of each level
   size_t J;              // bucket-reduction level-1 chunks per window
 };
 
@@ -61,10 +62,15 @@ Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false, in
   int per_thread = s.k0;
   s.levels = 0;
   while (true) {
+    // a level that fits one block spreads its records over every thread
+    // (its depth is the per-thread run plus the block tree)
+    if (s.levels > 0 && rec <= (size_t)seg_t * per_thread)
+      per_thread = std::max<int>(2, (int)((rec + seg_t - 1) / seg_t));
     size_t per_block = (size_t)seg_t * per_thread;
     size_t blocks = (rec + per_block - 1) / per_block;
     s.lvl_records[s.levels] = rec;
     s.lvl_blocks[s.levels] = blocks;
+    s.lvl_k[s.levels] = per_thread;
     s.levels++;
     if (blocks <= 1 || s.levels == 24) break;
     rec = 2 * blocks;
@@ -497,13 +503,14 @@ __global__ void __launch_bounds__(128) k_msm_reduce_l1(const xyzz<F>* __restrict
   st_pod(&acc_out[t], acc);
 }
 
-// block tree sum of one value per thread (result valid in thread 0)
+// block tree sum over the first `width` threads' values (a power of two;
+// result valid in thread 0)
 template <class F>
-__device__ __forceinline__ xyzz<F> block_sum(xyzz<F> v, xyzz<F>* sm) {
+__device__ __forceinline__ xyzz<F> block_sum(xyzz<F> v, xyzz<F>* sm, int width) {
   const int i = threadIdx.x;
   sm[i] = v;
   __syncthreads();
-  for (int s = kRedT / 2; s > 0; s >>= 1) {
+  for (int s = width / 2; s > 0; s >>= 1) {
     if (i < s) sm[i] = xyzz_add(sm[i], sm[i + s]);
     __syncthreads();
   }
@@ -512,7 +519,13 @@ __device__ __forceinline__ xyzz<F> block_sum(xyzz<F> v, xyzz<F>* sm) {
   return r;
 }
 
-// grid (segments, windows); out_u / out_a receive U and A of final passes
+// grid (segments, windows); out_u / out_a receive U and A of final passes.
+// Depth: the scan and the trees run over the segment's width (the power of
+// two covering its pairs), not the whole block.  When the doublings are few
+// (always between passes, and in a final pass when log_span + 1 is below the
+// tree depth) each thread folds 2^log_span S_i into its acc_i and one tree
+// sums the result, instead of two trees and a serial doubling tail; a final
+// pass then leaves U = infinity and the whole sum in A.
 template <class F>
 __global__ void __launch_bounds__(kRedT) k_msm_reduce_blk(
     const xyzz<F>* __restrict__ run_in, const xyzz<F>* __restrict__ acc_in, uint32_t Jin,
@@ -522,11 +535,17 @@ __global__ void __launch_bounds__(kRedT) k_msm_reduce_blk(
   const int w = blockIdx.y, i = threadIdx.x;
   const uint32_t idx = blockIdx.x * kRedT + i;
   const size_t base = (size_t)w * Jin;
+  const uint32_t len = min((uint32_t)kRedT, Jin - blockIdx.x * kRedT);
+  int width = 1, depth = 0;
+  while (width < (int)len) {
+    width <<= 1;
+    depth++;
+  }
   xyzz<F> r = idx < Jin ? ld_pod(run_in + base + idx) : xyzz_inf<F>();
   // inclusive suffix scan: r = S_i = sum_{k >= i} run_k within the segment
   sm[i] = r;
   __syncthreads();
-  for (int off = 1; off < kRedT; off <<= 1) {
+  for (int off = 1; off < width; off <<= 1) {
     const xyzz<F> o = i + off < kRedT ? sm[i + off] : xyzz_inf<F>();
     __syncthreads();
     r = xyzz_add(r, o);
@@ -535,19 +554,28 @@ __global__ void __launch_bounds__(kRedT) k_msm_reduce_blk(
   }
   const xyzz<F> total = sm[0];  // S_0 = sum of the segment's runs
   __syncthreads();
-  const xyzz<F> u = block_sum<F>(i >= 1 ? r : xyzz_inf<F>(), sm);
-  const xyzz<F> a = block_sum<F>(idx < Jin ? ld_pod(acc_in + base + idx) : xyzz_inf<F>(), sm);
-  if (i != 0) return;
-  if (Jout == 1) {
-    st_pod(&out_u[w], u);
-    st_pod(&out_a[w], a);
+  const xyzz<F> acc = idx < Jin ? ld_pod(acc_in + base + idx) : xyzz_inf<F>();
+  const size_t o = (size_t)w * Jout + blockIdx.x;
+  if (Jout > 1 || log_span + 1 < depth) {
+    xyzz<F> t = i >= 1 ? r : xyzz_inf<F>();
+    for (int d = 0; d < log_span; d++) t = xyzz_dbl(t);
+    const xyzz<F> s = block_sum<F>(xyzz_add(t, acc), sm, width);
+    if (i != 0) return;
+    if (Jout == 1) {
+      st_pod(&out_u[w], xyzz_inf<F>());
+      st_pod(&out_a[w], s);
+    } else {
+      st_pod(&run_out[o], total);
+      st_pod(&acc_out[o], s);
+    }
     return;
   }
-  xyzz<F> x = u;
-  for (int d = 0; d < log_span; d++) x = xyzz_dbl(x);
-  const size_t o = (size_t)w * Jout + blockIdx.x;
-  st_pod(&run_out[o], total);
-  st_pod(&acc_out[o], xyzz_add(a, x));
+  // final pass with many doublings: U and A separately, the host doubles U
+  const xyzz<F> u = block_sum<F>(i >= 1 ? r : xyzz_inf<F>(), sm, width);
+  const xyzz<F> a = block_sum<F>(acc, sm, width);
+  if (i != 0) return;
+  st_pod(&out_u[w], u);
+  st_pod(&out_a[w], a);
 }
 
 // ------------------------------------------------------ fixed-base tables
@@ -664,7 +692,7 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
     const int in = l & 1, out = in ^ 1;
     uint32_t* ok = (l + 1 < s.levels) ? L.pkey[out] : nullptr;
     k_msm_accumN<F><<<(unsigned)s.lvl_blocks[l], seg_threads<F>(), 0, st>>>(
-        L.pkey[in], L.ppt[in], s.lvl_records[l], s.k1, L.buckets, ok, L.ppt[out]);
+        L.pkey[in], L.ppt[in], s.lvl_records[l], s.lvl_k[l], L.buckets, ok, L.ppt[out]);
     ZK_LAUNCHED();
   }
   int log_span = 0;
