@@ -11,7 +11,9 @@
 //       waits for s2 and s3
 // so a group costs three MSM launch chains instead of four or five per
 // proof, and each chain is as large as the group: the load-balanced
-// accumulation and the bucket reduction see every job's records at once.
+// accumulation (persistent blocks pulling (instance, bucket-range) record
+// tiles from a device work queue) and the bucket reduction see every job's
+// records at once.
 // Each instance's window sum is exactly the single-MSM result, so proofs are
 // unchanged.
 // No reference counterpart (the reference proves one file pair per process).

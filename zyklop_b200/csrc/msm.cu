@@ -81,7 +81,8 @@ Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false, in
 
 template <class F>
 struct Layout {
-  uint32_t* counts;   // entries (exclusive offsets after the scan)
+  uint32_t* counts;   // entries (exclusive offsets after the scan), then the tile queue
+  uint32_t* tileq;    // work-queue counter of the persistent level 0 (counts[entries])
   uint32_t* cursor;   // entries
   uint32_t* tiles;    // scan tile sums
   uint32_t* skey;     // records
@@ -99,7 +100,8 @@ template <class F>
 Layout<F> carve(void* base, const Shape& s) {
   Layout<F> L{};
   Carver cv(base);
-  L.counts = cv.take<uint32_t>(s.entries);
+  L.counts = cv.take<uint32_t>(s.entries + 1);
+  L.tileq = L.counts + s.entries;
   L.cursor = cv.take<uint32_t>(s.entries);
   L.tiles = cv.take<uint32_t>(scan::tile_count(s.entries) + 1);
   L.skey = cv.take<uint32_t>(s.records);
@@ -321,7 +323,7 @@ __device__ __forceinline__ void seg_close(SegNode<F>& nd, const xyzz<F>& acc, ui
 template <class F>
 __device__ __forceinline__ void seg_block_finish(SegNode<F>* sm, uint32_t key_before,
                                                  uint32_t key_after, xyzz<F>* buckets,
-                                                 uint32_t* okey, xyzz<F>* opt) {
+                                                 uint32_t* okey, xyzz<F>* opt, size_t b) {
   constexpr int T = seg_threads<F>();
   const int t = threadIdx.x;
   __syncthreads();
@@ -332,7 +334,6 @@ __device__ __forceinline__ void seg_block_finish(SegNode<F>* sm, uint32_t key_be
   if (t != 0) return;
   const SegNode<F>& r = sm[0];
   uint32_t hk = kInvalid, tk = kInvalid;
-  const size_t b = blockIdx.x;
   if (r.fk != kInvalid) {
     const bool head = key_before == r.fk;
     if (r.single) {
@@ -378,19 +379,21 @@ struct PointSrc {
   const F* table[kMaxInst];   // fixed-base: record r of an instance at table + 2 r (x, y)
 };
 
-// Level 0: records are (bucket key, point index | sign) in bucket order.
+// Level 0, one tile: records [b T K, (b + 1) T K) of the list sorted by
+// (bucket key, point index | sign).
 template <class F, bool kFixed>
-__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
-    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
-    const uint32_t* __restrict__ total_p, const __grid_constant__ PointSrc<F> src, int K,
-    xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
+__device__ __forceinline__ void accum0_tile(size_t b, SegNode<F>* sm,
+                                            const uint32_t* __restrict__ skey,
+                                            const uint32_t* __restrict__ sval, size_t total,
+                                            const PointSrc<F>& src, int K,
+                                            xyzz<F>* __restrict__ buckets,
+                                            uint32_t* __restrict__ okey,
+                                            xyzz<F>* __restrict__ opt) {
   constexpr int T = seg_threads<F>();
-  __shared__ SegNode<F> sm[T];
   SegNode<F>& nd = sm[threadIdx.x];
   nd.fk = nd.lk = kInvalid;
   nd.single = 1;
-  const size_t total = *total_p;
-  const size_t bstart = (size_t)blockIdx.x * T * K;
+  const size_t bstart = b * T * K;
   const size_t bend = min(bstart + (size_t)T * K, total);
   uint32_t key_before = kInvalid, key_after = kInvalid;
   if (bstart < total) {
@@ -425,7 +428,40 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
     }
     seg_close(nd, acc, cur, buckets);
   }
-  seg_block_finish(sm, key_before, key_after, buckets, okey, opt);
+  seg_block_finish(sm, key_before, key_after, buckets, okey, opt, b);
+}
+
+// one tile per block
+template <class F, bool kFixed>
+__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
+    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
+    const uint32_t* __restrict__ total_p, const __grid_constant__ PointSrc<F> src, int K,
+    xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
+  __shared__ SegNode<F> sm[seg_threads<F>()];
+  accum0_tile<F, kFixed>(blockIdx.x, sm, skey, sval, *total_p, src, K, buckets, okey, opt);
+}
+
+// Persistent form for multi-instance chains (several proofs' MSMs): a grid
+// of as many blocks as the device holds at once, each claiming record tiles
+// (instance, bucket range) from a device work queue until all `ntiles` are
+// taken.  `queue` starts at zero.
+template <class F, bool kFixed>
+__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0_queue(
+    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
+    const uint32_t* __restrict__ total_p, const __grid_constant__ PointSrc<F> src, int K,
+    xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt,
+    uint32_t ntiles, uint32_t* __restrict__ queue) {
+  __shared__ SegNode<F> sm[seg_threads<F>()];
+  __shared__ uint32_t tile;
+  const size_t total = *total_p;
+  for (;;) {
+    __syncthreads();  // the previous tile's outputs (thread 0) are written
+    if (threadIdx.x == 0) tile = atomicAdd(queue, 1u);
+    __syncthreads();
+    const uint32_t b = tile;
+    if (b >= ntiles) return;
+    accum0_tile<F, kFixed>(b, sm, skey, sval, total, src, K, buckets, okey, opt);
+  }
 }
 
 // Levels >= 1: records are (bucket key, XYZZ partial sum); kInvalid keys
@@ -461,7 +497,7 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accumN(
     }
     seg_close(nd, acc, cur, buckets);
   }
-  seg_block_finish(sm, key_before, key_after, buckets, okey, opt);
+  seg_block_finish(sm, key_before, key_after, buckets, okey, opt, (size_t)blockIdx.x);
 }
 
 // ------------------------------------------------------ bucket reduction
@@ -637,6 +673,21 @@ __global__ void __launch_bounds__(128) k_msm_precompute(const F* __restrict__ px
 }
 
 
+// Blocks of the persistent level 0 the device holds at once.
+template <class F>
+int queue_grid() {
+  static const int g = [] {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_msm_accum0_queue<F, true>,
+                                                      seg_threads<F>(), 0) != cudaSuccess) {
+      (void)cudaGetLastError();
+      per_sm = 1;
+    }
+    return std::max(1, per_sm) * device_sm_count();
+  }();
+  return g;
+}
+
 // The GPU part of one launch chain: a windowed MSM (inst = 1, points from
 // ps.x / ps.y) or inst fixed-base MSMs of one window size sharing the chain
 // (tables in ps.table).  n_max: the largest instance, n_total: their sum.
@@ -656,7 +707,7 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
   Layout<F> L = carve<F>(scratch, s);
   ZK_REQUIRE(L.bytes <= scratch_bytes, ZK_EINVAL, "msm: scratch buffer too small");
 
-  ZK_CUDA(cudaMemsetAsync(L.counts, 0, s.entries * sizeof(uint32_t), st));
+  ZK_CUDA(cudaMemsetAsync(L.counts, 0, (s.entries + 1) * sizeof(uint32_t), st));
   ZK_CUDA(cudaMemsetAsync(L.buckets, 0, (size_t)s.Wk * s.B * sizeof(xyzz<F>), st));
   const int th = 256;
   const dim3 g((unsigned)((n_max + th - 1) / th), (unsigned)inst);
@@ -680,7 +731,12 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
   {
     uint32_t* ok = s.levels > 1 ? L.pkey[1] : nullptr;
     ProfScope prof(g2 ? kProfAccumG2 : kProfAccumG1, (double)n_total, st);
-    if (fixed)
+    if (fixed && inst > 1) {
+      const unsigned grid = (unsigned)std::min<size_t>(s.lvl_blocks[0], queue_grid<F>());
+      k_msm_accum0_queue<F, true><<<grid, seg_threads<F>(), 0, st>>>(
+          L.skey, L.sval, total_p, ps, s.k0, L.buckets, ok, L.ppt[1],
+          (uint32_t)s.lvl_blocks[0], L.tileq);
+    } else if (fixed)
       k_msm_accum0<F, true><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
           L.skey, L.sval, total_p, ps, s.k0, L.buckets, ok, L.ppt[1]);
     else

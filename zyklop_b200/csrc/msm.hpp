@@ -97,9 +97,11 @@ MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars,
 // Several fixed-base MSMs with the same window bits in one launch chain: one
 // instance per (table, scalars, n); their records share the sort, the
 // load-balanced accumulation and the bucket reduction (instance i's buckets
-// take the place of window i).  Scratch: msm_scratch_bytes_fixed(sum of n,
-// g2, c, cfg, inst).  The result holds one window sum per instance
-// (msm_g*_combine_inst).
+// take the place of window i).  Its level-0 accumulation is persistent: as
+// many blocks as the device holds at once claim record tiles (instance,
+// bucket range) from a device work queue.  Scratch:
+// msm_scratch_bytes_fixed(sum of n, g2, c, cfg, inst).  The result holds one
+// window sum per instance (msm_g*_combine_inst).
 constexpr int kMsmMaxInstances = 64;
 MsmResult msm_enqueue_fixed_multi(bool g2, int inst, const void* const* tables,
                                   const uint64_t* const* scalars, const size_t* n, int c,
