@@ -6,7 +6,8 @@
 //   after ev_staged, concurrently:
 //     s2: one multi-instance G2 MSM over every job's B2
 //     s3: one multi-instance G1 MSM over every job's A, C (and B1)
-//     sp[0..3]: SpMV + H polynomial per job, round robin
+//     sp[0..3]: SpMV per job and one batched H pipeline per run of
+//               same-size jobs (one launch per NTT stage for all of them)
 //   s1: (after sp[]) one multi-instance G1 MSM over every job's H, then
 //       waits for s2 and s3
 // so a group costs three MSM launch chains instead of four or five per
@@ -168,14 +169,34 @@ void fused_launch(zk_ctx* ctx, FusedWs& f, Group& g, const uint64_t* const* wits
   ZK_CUDA(cudaMemcpyAsync(f.win1w.ptr, g.rw.d_data, g.rw.bytes, cudaMemcpyDeviceToHost, f.s3));
   ZK_CUDA(cudaEventRecord(f.ev_g1w, f.s3));
 
-  // SpMV and H polynomial per job, round robin over the polynomial streams
-  const int np = (int)std::min<size_t>(nj, FusedWs::kPolyStreams);
+  // SpMV per job, then one H pipeline per run of same-size jobs (one launch
+  // per stage for all of them); each size is cut into up to kPolyStreams
+  // runs so the runs overlap on the polynomial streams
+  std::map<int, std::vector<size_t>> by_size;
+  for (size_t k = 0; k < nj; k++) by_size[g.jobs[k].c->log_n].push_back(k);
+  std::vector<std::vector<size_t>> runs;
+  for (auto& kv : by_size) {
+    const size_t m = kv.second.size();
+    const size_t per = std::min<size_t>(
+        kMaxHBatch, (m + FusedWs::kPolyStreams - 1) / FusedWs::kPolyStreams);
+    for (size_t a = 0; a < m; a += per)
+      runs.emplace_back(kv.second.begin() + a, kv.second.begin() + std::min(m, a + per));
+  }
+  const int np = (int)std::min<size_t>(runs.size(), FusedWs::kPolyStreams);
   for (int q = 0; q < np; q++) ZK_CUDA(cudaStreamWaitEvent(f.sp[q], f.ev_staged, 0));
-  for (size_t k = 0; k < nj; k++) {
-    zk_circuit* c = g.jobs[k].c;
-    cudaStream_t st = f.sp[k % FusedWs::kPolyStreams];
-    spmv_enqueue(c, we_of(k), poly_of(k, 0), poly_of(k, 1), st);
-    hpoly(ctx->ntt, poly_of(k, 0), poly_of(k, 1), poly_of(k, 2), c->log_n, poly_of(k, 3), st);
+  for (size_t ri = 0; ri < runs.size(); ri++) {
+    cudaStream_t st = f.sp[ri % FusedWs::kPolyStreams];
+    uint64_t *aw[kMaxHBatch], *bw[kMaxHBatch], *cw[kMaxHBatch], *hh[kMaxHBatch];
+    int cnt = 0;
+    for (size_t k : runs[ri]) {
+      spmv_enqueue(g.jobs[k].c, we_of(k), poly_of(k, 0), poly_of(k, 1), st);
+      aw[cnt] = poly_of(k, 0);
+      bw[cnt] = poly_of(k, 1);
+      cw[cnt] = poly_of(k, 2);
+      hh[cnt] = poly_of(k, 3);
+      cnt++;
+    }
+    hpoly_batch(ctx->ntt, cnt, aw, bw, cw, g.jobs[runs[ri][0]].c->log_n, hh, st);
   }
   for (int q = 0; q < np; q++) {
     ZK_CUDA(cudaEventRecord(f.ev_sp[q], f.sp[q]));

@@ -45,9 +45,20 @@ __global__ void k_tw_fill(fr_t* __restrict__ out, const fr_t* __restrict__ hi,
   fe_store(out, e, a * b);
 }
 
+// arrays transformed by one pass launch (blockIdx.y): the three vectors of
+// up to kMaxHBatch H polynomials of one size
+constexpr int kMaxPassArrays = 3 * kMaxHBatch;
 struct PassArgs {
-  fr_t* in[3];
-  fr_t* out[3];
+  fr_t* in[kMaxPassArrays];
+  fr_t* out[kMaxPassArrays];
+};
+
+// the vectors of up to kMaxHBatch H polynomials (blockIdx.y = polynomial)
+struct HArgs {
+  const fr_t* a[kMaxHBatch];
+  const fr_t* b[kMaxHBatch];
+  fr_t* c[kMaxHBatch];
+  fr_t* h[kMaxHBatch];
 };
 
 // One pass: radix-2 stages on global index bits [lo, lo + k) for every
@@ -148,10 +159,11 @@ __global__ void k_bitrev(const fr_t* __restrict__ in, fr_t* __restrict__ out, in
   fe_store(out, r, x);
 }
 
-__global__ void k_pointwise_mul(const fr_t* __restrict__ a, const fr_t* __restrict__ b,
-                                fr_t* __restrict__ c, size_t n) {
+// C = A * B elementwise, per polynomial
+__global__ void k_pointwise_mul(const __grid_constant__ HArgs args, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) fe_store(c, i, fe_load<FrCfg>(a, i) * fe_load<FrCfg>(b, i));
+  const int j = blockIdx.y;
+  if (i < n) fe_store(args.c[j], i, fe_load<FrCfg>(args.a[j], i) * fe_load<FrCfg>(args.b[j], i));
 }
 
 // x[p] *= (1/N) omega_2n^rev(p) for coefficients held in bit-reversed order
@@ -173,13 +185,15 @@ __global__ void k_coset_scale(PassArgs args, const fr_t* __restrict__ tw, int tw
   fe_store(a, p, fe_load<FrCfg>(a, p) * t * ((e & 1) ? c_odd : c_even));
 }
 
-// h = A*B - C, decoded to canonical (src/groth16.cu:935-948, 218-226)
-__global__ void k_h_final(const fr_t* __restrict__ a, const fr_t* __restrict__ b,
-                          const fr_t* __restrict__ c, fr_t* __restrict__ h, size_t n) {
+// h = A*B - C, decoded to canonical (src/groth16.cu:935-948, 218-226), per
+// polynomial
+__global__ void k_h_final(const __grid_constant__ HArgs args, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
   if (i >= n) return;
-  const fr_t v = fe_load<FrCfg>(a, i) * fe_load<FrCfg>(b, i) - fe_load<FrCfg>(c, i);
-  fe_store(h, i, fe_from_mont(v));
+  const fr_t v = fe_load<FrCfg>(args.a[j], i) * fe_load<FrCfg>(args.b[j], i) -
+                 fe_load<FrCfg>(args.c[j], i);
+  fe_store(args.h[j], i, fe_from_mont(v));
 }
 
 __global__ void k_fr_encode(const fr_t* __restrict__ in, fr_t* __restrict__ out, size_t n) {
@@ -306,27 +320,40 @@ void ntt_inplace(NttTables& tw, uint64_t* a, int log_n, bool inverse, void* scra
   ZK_LAUNCHED();
 }
 
-void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, uint64_t* h,
-           cudaStream_t st) {
+void hpoly_batch(NttTables& tw, int count, uint64_t* const* aw, uint64_t* const* bw,
+                 uint64_t* const* cw, int log_n, uint64_t* const* h, cudaStream_t st) {
   ZK_REQUIRE(log_n >= 1 && log_n < kMaxLogN, ZK_EINVAL, "hpoly: log_n out of range");
+  ZK_REQUIRE(count >= 1 && count <= kMaxHBatch, ZK_EINVAL, "hpoly: 1..16 polynomials per launch");
   tw.ensure(log_n, st);
   const size_t n = size_t(1) << log_n;
   const int shift = tw.lmax - log_n;
-  fr_t* A = reinterpret_cast<fr_t*>(aw);
-  fr_t* B = reinterpret_cast<fr_t*>(bw);
-  fr_t* C = reinterpret_cast<fr_t*>(cw);
-  k_pointwise_mul<<<blocks_for(n), 256, 0, st>>>(A, B, C, n);
+  HArgs ha{};
+  PassArgs abc{};
+  for (int j = 0; j < count; j++) {
+    ha.a[j] = reinterpret_cast<const fr_t*>(aw[j]);
+    ha.b[j] = reinterpret_cast<const fr_t*>(bw[j]);
+    ha.c[j] = reinterpret_cast<fr_t*>(cw[j]);
+    ha.h[j] = reinterpret_cast<fr_t*>(h[j]);
+    abc.in[3 * j] = abc.out[3 * j] = reinterpret_cast<fr_t*>(aw[j]);
+    abc.in[3 * j + 1] = abc.out[3 * j + 1] = reinterpret_cast<fr_t*>(bw[j]);
+    abc.in[3 * j + 2] = abc.out[3 * j + 2] = reinterpret_cast<fr_t*>(cw[j]);
+  }
+  k_pointwise_mul<<<dim3(blocks_for(n), count), 256, 0, st>>>(ha, n);
   ZK_LAUNCHED();
-  PassArgs abc{{A, B, C}, {A, B, C}};
-  dif(abc, abc, 3, tw.inv.as<fr_t>(), shift, log_n, tw.pass_bits[log_n], st);
+  dif(abc, abc, 3 * count, tw.inv.as<fr_t>(), shift, log_n, tw.pass_bits[log_n], st);
   const Fr ninv = Fr::from_u64(n).inv();
   const Fr c_odd = ninv * host_root(log_n + 1);
-  k_coset_scale<<<dim3(blocks_for(n), 3), 256, 0, st>>>(abc, tw.fwd.as<fr_t>(), shift, log_n,
-                                                        to_dev(ninv), to_dev(c_odd));
+  k_coset_scale<<<dim3(blocks_for(n), 3 * count), 256, 0, st>>>(abc, tw.fwd.as<fr_t>(), shift,
+                                                                log_n, to_dev(ninv), to_dev(c_odd));
   ZK_LAUNCHED();
-  dit(abc, 3, tw.fwd.as<fr_t>(), shift, log_n, tw.pass_bits[log_n], st);
-  k_h_final<<<blocks_for(n), 256, 0, st>>>(A, B, C, reinterpret_cast<fr_t*>(h), n);
+  dit(abc, 3 * count, tw.fwd.as<fr_t>(), shift, log_n, tw.pass_bits[log_n], st);
+  k_h_final<<<dim3(blocks_for(n), count), 256, 0, st>>>(ha, n);
   ZK_LAUNCHED();
+}
+
+void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, uint64_t* h,
+           cudaStream_t st) {
+  hpoly_batch(tw, 1, &aw, &bw, &cw, log_n, &h, st);
 }
 
 void fr_encode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t st) {

@@ -51,6 +51,11 @@ void ntt_inplace(NttTables& tw, uint64_t* a, int log_n, bool inverse, void* scra
 // same size; h receives canonical Fr.
 void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, uint64_t* h,
            cudaStream_t stream);
+// The same for `count` (1..kMaxHBatch) polynomials of one size in one
+// launch per stage (grid.y runs over the polynomials' vectors).
+constexpr int kMaxHBatch = 16;
+void hpoly_batch(NttTables& tw, int count, uint64_t* const* aw, uint64_t* const* bw,
+                 uint64_t* const* cw, int log_n, uint64_t* const* h, cudaStream_t stream);
 
 // Elementwise helpers over Montgomery / canonical Fr arrays.
 void fr_encode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t stream);
