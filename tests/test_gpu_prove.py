@@ -513,3 +513,22 @@ def test_fused_batch_needs_tables(api, files):
     finally:
         api.set_batch_mode(api.BATCH_AUTO, 16)
     assert np.array_equal(api.prove_batch([c], [wit])[0], c.prove(wit))
+
+
+def test_fused_group_at_the_instance_limit(api, files):
+    """32 unblinded jobs in one fused group: the A/C chain holds 64 instances,
+    the multi-instance maximum; every proof equals the single proof."""
+    c = api.Circuit(files["u10"][0])
+    c.precompute(10, 9)
+    wit = api.read_wtns(files["u10"][1])
+    single = c.prove(wit)
+    try:
+        api.set_batch_mode(api.BATCH_FUSED, 64)
+        proofs = api.prove_batch([c] * 32, [wit] * 32)
+        assert all(np.array_equal(p, single) for p in proofs)
+        # 33 jobs: a second group of one
+        proofs = api.prove_batch([c] * 33, [wit] * 33)
+        assert all(np.array_equal(p, single) for p in proofs)
+    finally:
+        api.set_batch_mode(api.BATCH_AUTO, 16)
+    c.close()
