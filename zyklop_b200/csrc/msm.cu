@@ -444,9 +444,10 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
 // Persistent form for multi-instance chains (several proofs' MSMs): a grid
 // of as many blocks as the device holds at once, each claiming record tiles
 // (instance, bucket range) from a device work queue until all `ntiles` are
-// taken.  `queue` starts at zero.
+// taken.  `queue` starts at zero.  Four blocks per SM, like the one-tile
+// form (the loop would otherwise cost the G1 kernel a block of residency).
 template <class F, bool kFixed>
-__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0_queue(
+__global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0_queue(
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
     const uint32_t* __restrict__ total_p, const __grid_constant__ PointSrc<F> src, int K,
     xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt,
