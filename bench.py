@@ -44,7 +44,10 @@ METRIC = "groth16_proofs_per_s"
 UNIT = "proofs/s"
 # algorithmic Fp multiplications per MSM point (bucket accumulation with the
 # reference's 16-window, 7M+4S mixed-add decomposition) and IMAD-class ops per
-# Fp multiplication (8x8 limb products lo+hi for a*b and m*p, plus m)
+# Fp multiplication (8x8 limb products lo+hi for a*b and m*p, plus m).  Both
+# are work conventions: the kernels issue 232 IMAD-class ops per Fp product
+# (Karatsuba) and 560 per Fp2 product (two reductions), so a fraction of the
+# carry-chain probe counted this way can exceed the issued one.
 FP_MULTS_PER_POINT = {"accum_g1": 176.0, "accum_g2": 528.0}
 IMAD_PER_FP_MULT = 264.0
 

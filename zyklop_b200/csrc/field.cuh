@@ -5,13 +5,17 @@
 // (include/fp_bn254.cuh:52-59, include/fr_bn254.cuh:40-49), so buffers cross
 // the API unchanged.  Values are kept fully reduced in [0, m).
 //
-// Multiplication is CIOS Montgomery with 32-bit limbs: each of the 8 rows is
-// two interleaved carry chains (even / odd limb products, mad.lo/madc.hi)
-// followed by the reduction row against the modulus, whose limbs are PTX
-// immediates.  Both BN254 moduli are below 2^254, so the 9-word accumulator
-// never overflows and no tenth carry word is kept (t + a*b_i + m*p < 2^288).
-// Replaces the reference's 4 x u64 CIOS fpMul / frMul
-// (include/fp_bn254.cuh:187-277, include/fr_bn254.cuh:173-210).
+// Multiplication is separated Montgomery with 32-bit limbs: the 512-bit
+// product comes from one level of Karatsuba over 128-bit halves (three 4 x 4
+// limb schoolbook products, 96 multiply instructions instead of 128), then
+// eight reduction rows against the modulus, whose limbs are PTX immediates,
+// fold the low half and the high half is added at the end.  Each schoolbook
+// or reduction row is two interleaved carry chains (even / odd limb
+// products, mad.lo/madc.hi).  Both BN254 moduli are below 2^254, which bounds
+// every intermediate (derivations at the functions).  The products are
+// bit-identical to the reference's 4 x u64 CIOS fpMul / frMul
+// (include/fp_bn254.cuh:187-277, include/fr_bn254.cuh:173-210): both return
+// the unique a*b*R^-1 mod m in [0, m).
 #pragma once
 #include <cstdint>
 
@@ -179,31 +183,6 @@ __device__ __forceinline__ fe<C> fe_dbl(const fe<C>& a) {
 }
 
 // ------------------------------------------------------------------- mul
-// t[0..8] += x[0..7] * y  (t8 receives the top word; never overflows here)
-#define ZK_ROW_EVEN(X0, X2, X4, X6, Y)                                                      \
-  asm("mad.lo.cc.u32  %0, %9, %13, %0;\n\t"                                                 \
-      "madc.hi.cc.u32 %1, %9, %13, %1;\n\t"                                                 \
-      "madc.lo.cc.u32 %2, %10, %13, %2;\n\t"                                                \
-      "madc.hi.cc.u32 %3, %10, %13, %3;\n\t"                                                \
-      "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"                                                \
-      "madc.hi.cc.u32 %5, %11, %13, %5;\n\t"                                                \
-      "madc.lo.cc.u32 %6, %12, %13, %6;\n\t"                                                \
-      "madc.hi.cc.u32 %7, %12, %13, %7;\n\t"                                                \
-      "addc.u32       %8, %8, 0;"                                                           \
-      : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), \
-        "+r"(t8)                                                                            \
-      : "r"(X0), "r"(X2), "r"(X4), "r"(X6), "r"(Y))
-#define ZK_ROW_ODD(X1, X3, X5, X7, Y)                                                       \
-  asm("mad.lo.cc.u32  %0, %8, %12, %0;\n\t"                                                 \
-      "madc.hi.cc.u32 %1, %8, %12, %1;\n\t"                                                 \
-      "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                 \
-      "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                 \
-      "madc.lo.cc.u32 %4, %10, %12, %4;\n\t"                                                \
-      "madc.hi.cc.u32 %5, %10, %12, %5;\n\t"                                                \
-      "madc.lo.cc.u32 %6, %11, %12, %6;\n\t"                                                \
-      "madc.hi.u32    %7, %11, %12, %7;"                                                    \
-      : "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)      \
-      : "r"(X1), "r"(X3), "r"(X5), "r"(X7), "r"(Y))
 // t += m * modulus, modulus limbs as immediates
 #define ZK_RED_EVEN(M)                                                                      \
   asm("mad.lo.cc.u32  %0, %13, %9, %0;\n\t"                                                 \
@@ -230,26 +209,197 @@ __device__ __forceinline__ fe<C> fe_dbl(const fe<C>& a) {
       : "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)      \
       : "n"(C::P1), "n"(C::P3), "n"(C::P5), "n"(C::P7), "r"(M))
 
-// Fully unrolled product (~300 instructions).  Kernels with one or two
-// products per loop body (NTT butterflies, SpMV, elementwise passes) call it
-// directly.
+// r[0..7] = x[0..3] * y[0..3].  Row j adds x * y_j at limb j as an even
+// chain (x0, x2) that also produces limb j+4 and an odd chain (x1, x3) that
+// ends there: the partial product after row j is below 2^(32(j+5)), so the
+// odd chain's last madc.hi never carries out.  Outputs are early-clobber:
+// they are written while inputs are still being read.
+__device__ __forceinline__ void mul_4x4(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3,
+                                        uint32_t y0, uint32_t y1, uint32_t y2, uint32_t y3,
+                                        uint32_t (&r)[8]) {
+  asm("mul.lo.u32     %0, %8, %12;\n\t"
+      "mul.hi.u32     %1, %8, %12;\n\t"
+      "mul.lo.u32     %2, %10, %12;\n\t"
+      "mul.hi.u32     %3, %10, %12;\n\t"
+      "mad.lo.cc.u32  %1, %9, %12, %1;\n\t"
+      "madc.hi.cc.u32 %2, %9, %12, %2;\n\t"
+      "madc.lo.cc.u32 %3, %11, %12, %3;\n\t"
+      "madc.hi.u32    %4, %11, %12, 0;\n\t"
+      "mad.lo.cc.u32  %1, %8, %13, %1;\n\t"
+      "madc.hi.cc.u32 %2, %8, %13, %2;\n\t"
+      "madc.lo.cc.u32 %3, %10, %13, %3;\n\t"
+      "madc.hi.cc.u32 %4, %10, %13, %4;\n\t"
+      "addc.u32       %5, 0, 0;\n\t"
+      "mad.lo.cc.u32  %2, %9, %13, %2;\n\t"
+      "madc.hi.cc.u32 %3, %9, %13, %3;\n\t"
+      "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"
+      "madc.hi.u32    %5, %11, %13, %5;\n\t"
+      "mad.lo.cc.u32  %2, %8, %14, %2;\n\t"
+      "madc.hi.cc.u32 %3, %8, %14, %3;\n\t"
+      "madc.lo.cc.u32 %4, %10, %14, %4;\n\t"
+      "madc.hi.cc.u32 %5, %10, %14, %5;\n\t"
+      "addc.u32       %6, 0, 0;\n\t"
+      "mad.lo.cc.u32  %3, %9, %14, %3;\n\t"
+      "madc.hi.cc.u32 %4, %9, %14, %4;\n\t"
+      "madc.lo.cc.u32 %5, %11, %14, %5;\n\t"
+      "madc.hi.u32    %6, %11, %14, %6;\n\t"
+      "mad.lo.cc.u32  %3, %8, %15, %3;\n\t"
+      "madc.hi.cc.u32 %4, %8, %15, %4;\n\t"
+      "madc.lo.cc.u32 %5, %10, %15, %5;\n\t"
+      "madc.hi.cc.u32 %6, %10, %15, %6;\n\t"
+      "addc.u32       %7, 0, 0;\n\t"
+      "mad.lo.cc.u32  %4, %9, %15, %4;\n\t"
+      "madc.hi.cc.u32 %5, %9, %15, %5;\n\t"
+      "madc.lo.cc.u32 %6, %11, %15, %6;\n\t"
+      "madc.hi.u32    %7, %11, %15, %7;"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]),
+        "=&r"(r[6]), "=&r"(r[7])
+      : "r"(x0), "r"(x1), "r"(x2), "r"(x3), "r"(y0), "r"(y1), "r"(y2), "r"(y3));
+}
+
+// T[0..15] = a * b for a, b < 2^255 (one Karatsuba level over 128-bit
+// halves): T = lo + (mid - lo - hi) 2^128 + hi 2^256 with lo = aL bL,
+// hi = aH bH, mid = (aL + aH)(bL + bH).  The half sums are 129-bit (carry
+// bits ca, cb), so mid is the 4 x 4 product of their low limbs plus
+// (ca sb + cb sa) 2^128 + ca cb 2^256, kept in nine limbs (mid < 2^258).
+// Order keeps few values live: mid first, then lo folded into T[0..12], then
+// hi added at 2^256 and subtracted at 2^128.  Every partial sum is a
+// nonnegative part of the product (mid - lo >= hi), so no chain borrows out,
+// and the largest, a b + hi 2^128 < 2^510 + 2^382, fits in 16 limbs (inputs
+// near 2^256 would not: field elements and unreduced sums of two stay below
+// 2^255).
+__device__ __forceinline__ void fe_mul_wide(const uint32_t (&a)[8], const uint32_t (&b)[8],
+                                            uint32_t (&T)[16]) {
+  uint32_t sa0, sa1, sa2, sa3, ca, sb0, sb1, sb2, sb3, cb;
+  asm("add.cc.u32  %0, %5, %9;\n\t"
+      "addc.cc.u32 %1, %6, %10;\n\t"
+      "addc.cc.u32 %2, %7, %11;\n\t"
+      "addc.cc.u32 %3, %8, %12;\n\t"
+      "addc.u32    %4, 0, 0;"
+      : "=r"(sa0), "=r"(sa1), "=r"(sa2), "=r"(sa3), "=r"(ca)
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]));
+  asm("add.cc.u32  %0, %5, %9;\n\t"
+      "addc.cc.u32 %1, %6, %10;\n\t"
+      "addc.cc.u32 %2, %7, %11;\n\t"
+      "addc.cc.u32 %3, %8, %12;\n\t"
+      "addc.u32    %4, 0, 0;"
+      : "=r"(sb0), "=r"(sb1), "=r"(sb2), "=r"(sb3), "=r"(cb)
+      : "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+  uint32_t mid[8], m8;
+  mul_4x4(sa0, sa1, sa2, sa3, sb0, sb1, sb2, sb3, mid);
+  const uint32_t ma = 0u - ca, mb = 0u - cb;
+  asm("add.cc.u32  %0, %0, %5;\n\t"
+      "addc.cc.u32 %1, %1, %6;\n\t"
+      "addc.cc.u32 %2, %2, %7;\n\t"
+      "addc.cc.u32 %3, %3, %8;\n\t"
+      "addc.u32    %4, 0, 0;"
+      : "+r"(mid[4]), "+r"(mid[5]), "+r"(mid[6]), "+r"(mid[7]), "=r"(m8)
+      : "r"(sb0 & ma), "r"(sb1 & ma), "r"(sb2 & ma), "r"(sb3 & ma));
+  asm("add.cc.u32  %0, %0, %5;\n\t"
+      "addc.cc.u32 %1, %1, %6;\n\t"
+      "addc.cc.u32 %2, %2, %7;\n\t"
+      "addc.cc.u32 %3, %3, %8;\n\t"
+      "addc.u32    %4, %4, %9;"
+      : "+r"(mid[4]), "+r"(mid[5]), "+r"(mid[6]), "+r"(mid[7]), "+r"(m8)
+      : "r"(sa0 & mb), "r"(sa1 & mb), "r"(sa2 & mb), "r"(sa3 & mb), "r"(ca & cb));
+  // lo: T[0..12] = lo + (mid - lo) 2^128
+  uint32_t w[8];
+  mul_4x4(a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3], w);
+  asm("sub.cc.u32  %0, %0, %9;\n\t"
+      "subc.cc.u32 %1, %1, %10;\n\t"
+      "subc.cc.u32 %2, %2, %11;\n\t"
+      "subc.cc.u32 %3, %3, %12;\n\t"
+      "subc.cc.u32 %4, %4, %13;\n\t"
+      "subc.cc.u32 %5, %5, %14;\n\t"
+      "subc.cc.u32 %6, %6, %15;\n\t"
+      "subc.cc.u32 %7, %7, %16;\n\t"
+      "subc.u32    %8, %8, 0;"
+      : "+r"(mid[0]), "+r"(mid[1]), "+r"(mid[2]), "+r"(mid[3]), "+r"(mid[4]), "+r"(mid[5]),
+        "+r"(mid[6]), "+r"(mid[7]), "+r"(m8)
+      : "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]));
+  T[0] = w[0]; T[1] = w[1]; T[2] = w[2]; T[3] = w[3];
+  asm("add.cc.u32  %0, %9, %13;\n\t"
+      "addc.cc.u32 %1, %10, %14;\n\t"
+      "addc.cc.u32 %2, %11, %15;\n\t"
+      "addc.cc.u32 %3, %12, %16;\n\t"
+      "addc.cc.u32 %4, %17, 0;\n\t"
+      "addc.cc.u32 %5, %18, 0;\n\t"
+      "addc.cc.u32 %6, %19, 0;\n\t"
+      "addc.cc.u32 %7, %20, 0;\n\t"
+      "addc.u32    %8, %21, 0;"
+      : "=r"(T[4]), "=r"(T[5]), "=r"(T[6]), "=r"(T[7]), "=r"(T[8]), "=r"(T[9]), "=r"(T[10]),
+        "=r"(T[11]), "=r"(T[12])
+      : "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(mid[0]), "r"(mid[1]), "r"(mid[2]),
+        "r"(mid[3]), "r"(mid[4]), "r"(mid[5]), "r"(mid[6]), "r"(mid[7]), "r"(m8));
+  // hi: add at 2^256, subtract at 2^128
+  mul_4x4(a[4], a[5], a[6], a[7], b[4], b[5], b[6], b[7], w);
+  asm("add.cc.u32  %0, %0, %8;\n\t"
+      "addc.cc.u32 %1, %1, %9;\n\t"
+      "addc.cc.u32 %2, %2, %10;\n\t"
+      "addc.cc.u32 %3, %3, %11;\n\t"
+      "addc.cc.u32 %4, %4, %12;\n\t"
+      "addc.cc.u32 %5, %13, 0;\n\t"
+      "addc.cc.u32 %6, %14, 0;\n\t"
+      "addc.u32    %7, %15, 0;"
+      : "+r"(T[8]), "+r"(T[9]), "+r"(T[10]), "+r"(T[11]), "+r"(T[12]), "=r"(T[13]), "=r"(T[14]),
+        "=r"(T[15])
+      : "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]));
+  asm("sub.cc.u32  %0, %0, %12;\n\t"
+      "subc.cc.u32 %1, %1, %13;\n\t"
+      "subc.cc.u32 %2, %2, %14;\n\t"
+      "subc.cc.u32 %3, %3, %15;\n\t"
+      "subc.cc.u32 %4, %4, %16;\n\t"
+      "subc.cc.u32 %5, %5, %17;\n\t"
+      "subc.cc.u32 %6, %6, %18;\n\t"
+      "subc.cc.u32 %7, %7, %19;\n\t"
+      "subc.cc.u32 %8, %8, 0;\n\t"
+      "subc.cc.u32 %9, %9, 0;\n\t"
+      "subc.cc.u32 %10, %10, 0;\n\t"
+      "subc.u32    %11, %11, 0;"
+      : "+r"(T[4]), "+r"(T[5]), "+r"(T[6]), "+r"(T[7]), "+r"(T[8]), "+r"(T[9]), "+r"(T[10]),
+        "+r"(T[11]), "+r"(T[12]), "+r"(T[13]), "+r"(T[14]), "+r"(T[15])
+      : "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]));
+}
+
+// Montgomery reduction T * 2^-256 mod m for T < 2^256 * m / 2 (fully reduced
+// result).  Eight rows fold the low half: starting from t = T_lo < 2^256, row i
+// adds q_i * m (q_i = t_0 * (-m^-1) mod 2^32) and shifts one word down, so
+// t < 2^256 + 2^32 m stays within nine words and ends at (T_lo + q m) / 2^256
+// <= m.  Adding T_hi < m/2 gives < 2m; one conditional subtraction finishes.
 template <class C>
-__device__ __forceinline__ fe<C> fe_mul_inline(const fe<C>& a, const fe<C>& b) {
-  uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0;
+__device__ __forceinline__ fe<C> fe_redc(const uint32_t (&T)[16]) {
+  uint32_t t0 = T[0], t1 = T[1], t2 = T[2], t3 = T[3], t4 = T[4], t5 = T[5], t6 = T[6], t7 = T[7];
+  uint32_t t8 = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    const uint32_t bi = b.v[i];
-    ZK_ROW_EVEN(a.v[0], a.v[2], a.v[4], a.v[6], bi);
-    ZK_ROW_ODD(a.v[1], a.v[3], a.v[5], a.v[7], bi);
     const uint32_t m = t0 * C::INV;
     ZK_RED_EVEN(m);
     ZK_RED_ODD(m);
-    // t0 is now zero: shift one word down
     t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = t5; t5 = t6; t6 = t7; t7 = t8; t8 = 0;
   }
-  fe<C> r{{t0, t1, t2, t3, t4, t5, t6, t7}};
+  fe<C> r;
+  asm("add.cc.u32  %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32    %7, %15, %23;"
+      : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]),
+        "=r"(r.v[6]), "=r"(r.v[7])
+      : "r"(t0), "r"(t1), "r"(t2), "r"(t3), "r"(t4), "r"(t5), "r"(t6), "r"(t7), "r"(T[8]),
+        "r"(T[9]), "r"(T[10]), "r"(T[11]), "r"(T[12]), "r"(T[13]), "r"(T[14]), "r"(T[15]));
   fe_reduce_once<C>(r.v);
   return r;
+}
+
+// Full product: a, b < m give T < m^2 < 2^256 * m / 4.
+template <class C>
+__device__ __forceinline__ fe<C> fe_mul_inline(const fe<C>& a, const fe<C>& b) {
+  uint32_t T[16];
+  fe_mul_wide(a.v, b.v, T);
+  return fe_redc<C>(T);
 }
 
 // Out-of-line product (arguments and result travel in registers).  Curve
@@ -313,11 +463,99 @@ struct fp2_t {
 
 __device__ __forceinline__ fp2_t operator+(const fp2_t& a, const fp2_t& b) { return {a.c0 + b.c0, a.c1 + b.c1}; }
 __device__ __forceinline__ fp2_t operator-(const fp2_t& a, const fp2_t& b) { return {a.c0 - b.c0, a.c1 - b.c1}; }
+
+// x[0..15] -= y[0..15]; the caller guarantees x >= y.
+__device__ __forceinline__ void sub_16(uint32_t (&x)[16], const uint32_t (&y)[16]) {
+  asm("sub.cc.u32  %0, %0, %16;\n\t"
+      "subc.cc.u32 %1, %1, %17;\n\t"
+      "subc.cc.u32 %2, %2, %18;\n\t"
+      "subc.cc.u32 %3, %3, %19;\n\t"
+      "subc.cc.u32 %4, %4, %20;\n\t"
+      "subc.cc.u32 %5, %5, %21;\n\t"
+      "subc.cc.u32 %6, %6, %22;\n\t"
+      "subc.cc.u32 %7, %7, %23;\n\t"
+      "subc.cc.u32 %8, %8, %24;\n\t"
+      "subc.cc.u32 %9, %9, %25;\n\t"
+      "subc.cc.u32 %10, %10, %26;\n\t"
+      "subc.cc.u32 %11, %11, %27;\n\t"
+      "subc.cc.u32 %12, %12, %28;\n\t"
+      "subc.cc.u32 %13, %13, %29;\n\t"
+      "subc.cc.u32 %14, %14, %30;\n\t"
+      "subc.u32    %15, %15, %31;"
+      : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]),
+        "+r"(x[7]), "+r"(x[8]), "+r"(x[9]), "+r"(x[10]), "+r"(x[11]), "+r"(x[12]), "+r"(x[13]),
+        "+r"(x[14]), "+r"(x[15])
+      : "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]), "r"(y[4]), "r"(y[5]), "r"(y[6]), "r"(y[7]),
+        "r"(y[8]), "r"(y[9]), "r"(y[10]), "r"(y[11]), "r"(y[12]), "r"(y[13]), "r"(y[14]),
+        "r"(y[15]));
+}
+
+// y = x + p^2 (p the base-field modulus; x < 2^508 so no carry out).
+__device__ __forceinline__ void add_16_psq(const uint32_t (&x)[16], uint32_t (&y)[16]) {
+  asm("add.cc.u32  %0, %16, 0x275d69b1;\n\t"
+      "addc.cc.u32 %1, %17, 0x3b5458a2;\n\t"
+      "addc.cc.u32 %2, %18, 0x09eac101;\n\t"
+      "addc.cc.u32 %3, %19, 0xa602072d;\n\t"
+      "addc.cc.u32 %4, %20, 0x6d96cadc;\n\t"
+      "addc.cc.u32 %5, %21, 0x4a50189c;\n\t"
+      "addc.cc.u32 %6, %22, 0x7a1242c8;\n\t"
+      "addc.cc.u32 %7, %23, 0x04689e95;\n\t"
+      "addc.cc.u32 %8, %24, 0x34c6b38d;\n\t"
+      "addc.cc.u32 %9, %25, 0x26edfa5c;\n\t"
+      "addc.cc.u32 %10, %26, 0x16375606;\n\t"
+      "addc.cc.u32 %11, %27, 0xb00b8551;\n\t"
+      "addc.cc.u32 %12, %28, 0x0348d21c;\n\t"
+      "addc.cc.u32 %13, %29, 0x599a6f7c;\n\t"
+      "addc.cc.u32 %14, %30, 0x763cbf9c;\n\t"
+      "addc.u32    %15, %31, 0x0925c4b8;"
+      : "=r"(y[0]), "=r"(y[1]), "=r"(y[2]), "=r"(y[3]), "=r"(y[4]), "=r"(y[5]), "=r"(y[6]),
+        "=r"(y[7]), "=r"(y[8]), "=r"(y[9]), "=r"(y[10]), "=r"(y[11]), "=r"(y[12]), "=r"(y[13]),
+        "=r"(y[14]), "=r"(y[15])
+      : "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(x[4]), "r"(x[5]), "r"(x[6]), "r"(x[7]),
+        "r"(x[8]), "r"(x[9]), "r"(x[10]), "r"(x[11]), "r"(x[12]), "r"(x[13]), "r"(x[14]),
+        "r"(x[15]));
+}
+
+// s = a + b without reduction (a, b < p give s < 2p < 2^255).
+__device__ __forceinline__ void add_raw(const uint32_t (&a)[8], const uint32_t (&b)[8],
+                                        uint32_t (&s)[8]) {
+  asm("add.cc.u32  %0, %8, %16;\n\t"
+      "addc.cc.u32 %1, %9, %17;\n\t"
+      "addc.cc.u32 %2, %10, %18;\n\t"
+      "addc.cc.u32 %3, %11, %19;\n\t"
+      "addc.cc.u32 %4, %12, %20;\n\t"
+      "addc.cc.u32 %5, %13, %21;\n\t"
+      "addc.cc.u32 %6, %14, %22;\n\t"
+      "addc.u32    %7, %15, %23;"
+      : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]),
+        "=r"(s[7])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+        "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+}
+
+// (a0 + a1 u)(b0 + b1 u) with two reductions instead of three (Karatsuba over
+// Fp2 on unreduced 512-bit products):
+//   c0 = REDC(a0 b0 - a1 b1 + p^2),  c1 = REDC((a0 + a1)(b0 + b1) - a0 b0 - a1 b1).
+// Both REDC arguments lie in [0, 2 p^2), below the 2^256 p / 2 that fe_redc
+// needs (p < 2^254); adding p^2 changes nothing mod p.  Same result as three
+// reduced products (the reference's fp2Mul, include/fp2_bn254.cuh:96-180).
+// Out of line like fe_mul_call, so the curve formulas share one body.
+static __device__ __noinline__ fp2_t fp2_mul_call(fp2_t a, fp2_t b) {
+  uint32_t s[8], t[8], x[16], y[16], w[16];
+  add_raw(a.c0.v, a.c1.v, s);
+  add_raw(b.c0.v, b.c1.v, t);
+  fe_mul_wide(s, t, x);
+  fe_mul_wide(a.c0.v, b.c0.v, w);
+  sub_16(x, w);
+  add_16_psq(w, y);
+  fe_mul_wide(a.c1.v, b.c1.v, w);
+  sub_16(x, w);
+  sub_16(y, w);
+  return {fe_redc<FpCfg>(y), fe_redc<FpCfg>(x)};
+}
+
 __device__ __forceinline__ fp2_t operator*(const fp2_t& a, const fp2_t& b) {
-  // Karatsuba: 3 base-field multiplications
-  fp_t t0 = a.c0 * b.c0, t1 = a.c1 * b.c1;
-  fp_t t2 = (a.c0 + a.c1) * (b.c0 + b.c1);
-  return {t0 - t1, t2 - t0 - t1};
+  return fp2_mul_call(a, b);
 }
 __device__ __forceinline__ fp2_t fe_sqr(const fp2_t& a) {
   // (c0 + c1)(c0 - c1) + 2 c0 c1 u: 2 multiplications
