@@ -50,7 +50,7 @@ __device__ __forceinline__ xyzz<F> xyzz_dbl(const xyzz<F>& p) {
   F m = fe_triple(fe_sqr(p.x));
   xyzz<F> r;
   r.x = fe_sqr(m) - fe_dbl(s);
-  r.y = m * (s - r.x) - w * p.y;
+  r.y = fe_mul_sub(m, s - r.x, w, p.y);
   r.zz = v * p.zz;
   r.zzz = w * p.zzz;
   return r;
@@ -66,7 +66,7 @@ __device__ __forceinline__ xyzz<F> xyzz_mdbl(const F& x, const F& y) {
   F m = fe_triple(fe_sqr(x));
   xyzz<F> r;
   r.x = fe_sqr(m) - fe_dbl(s);
-  r.y = m * (s - r.x) - w * y;
+  r.y = fe_mul_sub(m, s - r.x, w, y);
   r.zz = v;
   r.zzz = w;
   return r;
@@ -89,7 +89,7 @@ __device__ __forceinline__ xyzz<F> xyzz_madd(const xyzz<F>& p, const F& x, const
   F q = p.x * pp;
   xyzz<F> r;
   r.x = fe_sqr(rr) - ppp - fe_dbl(q);
-  r.y = rr * (q - r.x) - p.y * ppp;
+  r.y = fe_mul_sub(rr, q - r.x, p.y, ppp);
   r.zz = p.zz * pp;
   r.zzz = p.zzz * ppp;
   return r;
@@ -115,7 +115,7 @@ __device__ __forceinline__ xyzz<F> xyzz_add(const xyzz<F>& p, const xyzz<F>& q) 
   F qq = u1 * pp;
   xyzz<F> r;
   r.x = fe_sqr(rr) - ppp - fe_dbl(qq);
-  r.y = rr * (qq - r.x) - s1 * ppp;
+  r.y = fe_mul_sub(rr, qq - r.x, s1, ppp);
   r.zz = p.zz * q.zz * pp;
   r.zzz = p.zzz * q.zzz * ppp;
   return r;

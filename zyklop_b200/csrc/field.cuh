@@ -361,11 +361,11 @@ __device__ __forceinline__ void fe_mul_wide(const uint32_t (&a)[8], const uint32
       : "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]));
 }
 
-// Montgomery reduction T * 2^-256 mod m for T < 2^256 * m / 2 (fully reduced
+// Montgomery reduction T * 2^-256 mod m for T < 2^256 * m (fully reduced
 // result).  Eight rows fold the low half: starting from t = T_lo < 2^256, row i
 // adds q_i * m (q_i = t_0 * (-m^-1) mod 2^32) and shifts one word down, so
 // t < 2^256 + 2^32 m stays within nine words and ends at (T_lo + q m) / 2^256
-// <= m.  Adding T_hi < m/2 gives < 2m; one conditional subtraction finishes.
+// <= m.  Adding T_hi < m gives < 2m; one conditional subtraction finishes.
 template <class C>
 __device__ __forceinline__ fe<C> fe_redc(const uint32_t (&T)[16]) {
   uint32_t t0 = T[0], t1 = T[1], t2 = T[2], t3 = T[3], t4 = T[4], t5 = T[5], t6 = T[6], t7 = T[7];
@@ -490,7 +490,7 @@ __device__ __forceinline__ void sub_16(uint32_t (&x)[16], const uint32_t (&y)[16
         "r"(y[15]));
 }
 
-// y = x + p^2 (p the base-field modulus; x < 2^508 so no carry out).
+// y = x + p^2 (p the base-field modulus; every caller's x + p^2 < 2^512).
 __device__ __forceinline__ void add_16_psq(const uint32_t (&x)[16], uint32_t (&y)[16]) {
   asm("add.cc.u32  %0, %16, 0x275d69b1;\n\t"
       "addc.cc.u32 %1, %17, 0x3b5458a2;\n\t"
@@ -557,6 +557,32 @@ static __device__ __noinline__ fp2_t fp2_mul_call(fp2_t a, fp2_t b) {
 __device__ __forceinline__ fp2_t operator*(const fp2_t& a, const fp2_t& b) {
   return fp2_mul_call(a, b);
 }
+
+// a b - c d in Fp with one reduction: REDC(a b + p^2 - c d), whose argument
+// lies in (0, 2 p^2).  The Y coordinate of every XYZZ addition and doubling
+// has this shape (Y3 = R (Q - X3) - Y1 PPP).
+static __device__ __noinline__ fp_t fp_mul_sub_call(fp_t a, fp_t b, fp_t c, fp_t d) {
+  uint32_t x[16], w[16];
+  fe_mul_wide(a.v, b.v, w);
+  add_16_psq(w, x);
+  fe_mul_wide(c.v, d.v, w);
+  sub_16(x, w);
+  return fe_redc<FpCfg>(x);
+}
+
+__device__ __forceinline__ fp_t fe_mul_sub(const fp_t& a, const fp_t& b, const fp_t& c,
+                                           const fp_t& d) {
+  return fp_mul_sub_call(a, b, c, d);
+}
+
+// In Fp2 the same sharing (two reductions instead of four) keeps three
+// 512-bit accumulators beside four Fp2 operands; the G2 kernels spilled and
+// ran slower, so the Fp2 form stays two products and a subtraction.
+__device__ __forceinline__ fp2_t fe_mul_sub(const fp2_t& a, const fp2_t& b, const fp2_t& c,
+                                            const fp2_t& d) {
+  return a * b - c * d;
+}
+
 __device__ __forceinline__ fp2_t fe_sqr(const fp2_t& a) {
   // (c0 + c1)(c0 - c1) + 2 c0 c1 u: 2 multiplications
   fp_t t = a.c0 * a.c1;
