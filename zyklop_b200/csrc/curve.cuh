@@ -72,7 +72,9 @@ __device__ __forceinline__ xyzz<F> xyzz_mdbl(const F& x, const F& y) {
   return r;
 }
 
-// p + (x, y) for an affine point that is not the point at infinity
+// p + (x, y) for an affine point that is not the point at infinity.  ZZ3
+// and ZZZ3 are formed before X3 and Y3 so that ZZ1, ZZZ1 and PP die early
+// (fewer live registers in the accumulation loops).
 template <class F>
 __device__ __forceinline__ xyzz<F> xyzz_madd(const xyzz<F>& p, const F& x, const F& y) {
   if (xyzz_is_inf(p)) return {x, y, fe_one_of<F>(), fe_one_of<F>()};
@@ -88,10 +90,10 @@ __device__ __forceinline__ xyzz<F> xyzz_madd(const xyzz<F>& p, const F& x, const
   F ppp = pp_ * pp;
   F q = p.x * pp;
   xyzz<F> r;
-  r.x = fe_sqr(rr) - ppp - fe_dbl(q);
-  r.y = fe_mul_sub(rr, q - r.x, p.y, ppp);
   r.zz = p.zz * pp;
   r.zzz = p.zzz * ppp;
+  r.x = fe_sqr(rr) - ppp - fe_dbl(q);
+  r.y = fe_mul_sub(rr, q - r.x, p.y, ppp);
   return r;
 }
 
@@ -114,10 +116,10 @@ __device__ __forceinline__ xyzz<F> xyzz_add(const xyzz<F>& p, const xyzz<F>& q) 
   F ppp = pp_ * pp;
   F qq = u1 * pp;
   xyzz<F> r;
-  r.x = fe_sqr(rr) - ppp - fe_dbl(qq);
-  r.y = fe_mul_sub(rr, qq - r.x, s1, ppp);
   r.zz = p.zz * q.zz * pp;
   r.zzz = p.zzz * q.zzz * ppp;
+  r.x = fe_sqr(rr) - ppp - fe_dbl(qq);
+  r.y = fe_mul_sub(rr, qq - r.x, s1, ppp);
   return r;
 }
 
