@@ -85,8 +85,7 @@ struct Layout {
   uint32_t* tileq;    // work-queue counter of the persistent level 0 (counts[entries])
   uint32_t* cursor;   // entries
   uint32_t* tiles;    // scan tile sums
-  uint32_t* skey;     // records
-  uint32_t* sval;     // records
+  uint2* srec;        // records: (bucket key, point index | sign), one 8-byte store each
   xyzz<F>* buckets;   // W*B
   uint32_t* pkey[2];  // ping-pong partial records
   xyzz<F>* ppt[2];
@@ -104,8 +103,7 @@ Layout<F> carve(void* base, const Shape& s) {
   L.tileq = L.counts + s.entries;
   L.cursor = cv.take<uint32_t>(s.entries);
   L.tiles = cv.take<uint32_t>(scan::tile_count(s.entries) + 1);
-  L.skey = cv.take<uint32_t>(s.records);
-  L.sval = cv.take<uint32_t>(s.records);
+  L.srec = cv.take<uint2>(s.records);
   L.buckets = cv.take<xyzz<F>>((size_t)s.Wk * s.B);
   size_t pmax[2] = {1, 1};
   for (int l = 1; l < s.levels; l++) pmax[l & 1] = std::max(pmax[l & 1], s.lvl_records[l]);
@@ -220,8 +218,7 @@ __global__ void k_msm_hist(const __grid_constant__ ScalarSrc src, int c, int W, 
 
 template <bool kFixed>
 __global__ void k_msm_scatter(const __grid_constant__ ScalarSrc src, int c, int W, uint32_t B,
-                              uint32_t* __restrict__ cursor, uint32_t* __restrict__ skey,
-                              uint32_t* __restrict__ sval) {
+                              uint32_t* __restrict__ cursor, uint2* __restrict__ srec) {
   const int inst = blockIdx.y;
   const uint32_t n = src.n[inst];
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -243,9 +240,8 @@ __global__ void k_msm_scatter(const __grid_constant__ ScalarSrc src, int c, int 
     base = __shfl_sync(0xffffffffu, base, leader);
     if (key != kInvalid) {
       const uint32_t pos = base + __popc(peers & lt);
-      skey[pos] = key;
       const uint32_t idx = kFixed ? (uint32_t)((size_t)w * n + i) : (uint32_t)i;
-      sval[pos] = idx | (neg ? kNeg : 0u);
+      srec[pos] = make_uint2(key, idx | (neg ? kNeg : 0u));
     }
   }
 }
@@ -383,8 +379,7 @@ struct PointSrc {
 // (bucket key, point index | sign).
 template <class F, bool kFixed>
 __device__ __forceinline__ void accum0_tile(size_t b, SegNode<F>* sm,
-                                            const uint32_t* __restrict__ skey,
-                                            const uint32_t* __restrict__ sval, size_t total,
+                                            const uint2* __restrict__ srec, size_t total,
                                             const PointSrc<F>& src, int K,
                                             xyzz<F>* __restrict__ buckets,
                                             uint32_t* __restrict__ okey,
@@ -397,20 +392,21 @@ __device__ __forceinline__ void accum0_tile(size_t b, SegNode<F>* sm,
   const size_t bend = min(bstart + (size_t)T * K, total);
   uint32_t key_before = kInvalid, key_after = kInvalid;
   if (bstart < total) {
-    key_before = bstart ? skey[bstart - 1] : kInvalid;
-    key_after = bend < total ? skey[bend] : kInvalid;
+    key_before = bstart ? srec[bstart - 1].x : kInvalid;
+    key_after = bend < total ? srec[bend].x : kInvalid;
     const size_t s = bstart + (size_t)threadIdx.x * K;
     const size_t e = min(s + K, bend);
     xyzz<F> acc = xyzz_inf<F>();
     uint32_t cur = kInvalid;
     for (size_t p = s; p < e; p++) {
-      const uint32_t key = skey[p];
+      const uint2 rec = srec[p];
+      const uint32_t key = rec.x;
       if (key != cur) {
         seg_close(nd, acc, cur, buckets);
         cur = key;
         acc = xyzz_inf<F>();
       }
-      const uint32_t v = sval[p];
+      const uint32_t v = rec.y;
       const uint32_t idx = v & ~kNeg;
       F x, y;
       if (kFixed) {
@@ -437,11 +433,11 @@ __device__ __forceinline__ void accum0_tile(size_t b, SegNode<F>* sm,
 // 255-register limit either way.
 template <class F, bool kFixed>
 __global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0(
-    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
-    const uint32_t* __restrict__ total_p, const __grid_constant__ PointSrc<F> src, int K,
+    const uint2* __restrict__ srec, const uint32_t* __restrict__ total_p,
+    const __grid_constant__ PointSrc<F> src, int K,
     xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
   __shared__ SegNode<F> sm[seg_threads<F>()];
-  accum0_tile<F, kFixed>(blockIdx.x, sm, skey, sval, *total_p, src, K, buckets, okey, opt);
+  accum0_tile<F, kFixed>(blockIdx.x, sm, srec, *total_p, src, K, buckets, okey, opt);
 }
 
 // Persistent form for multi-instance chains (several proofs' MSMs): a grid
@@ -451,8 +447,8 @@ __global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0(
 // form.
 template <class F, bool kFixed>
 __global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0_queue(
-    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sval,
-    const uint32_t* __restrict__ total_p, const __grid_constant__ PointSrc<F> src, int K,
+    const uint2* __restrict__ srec, const uint32_t* __restrict__ total_p,
+    const __grid_constant__ PointSrc<F> src, int K,
     xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt,
     uint32_t ntiles, uint32_t* __restrict__ queue) {
   __shared__ SegNode<F> sm[seg_threads<F>()];
@@ -464,7 +460,7 @@ __global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0_queue(
     __syncthreads();
     const uint32_t b = tile;
     if (b >= ntiles) return;
-    accum0_tile<F, kFixed>(b, sm, skey, sval, total, src, K, buckets, okey, opt);
+    accum0_tile<F, kFixed>(b, sm, srec, total, src, K, buckets, okey, opt);
   }
 }
 
@@ -725,9 +721,9 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
   scan::exclusive(L.counts, L.cursor, s.entries, L.tiles, st);
   if (n_max) {
     if (fixed)
-      k_msm_scatter<true><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
+      k_msm_scatter<true><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.cursor, L.srec);
     else
-      k_msm_scatter<false><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.cursor, L.skey, L.sval);
+      k_msm_scatter<false><<<g, th, 0, st>>>(ss, s.c, s.W, s.B, L.cursor, L.srec);
     ZK_LAUNCHED();
   }
   const uint32_t* total_p = L.counts + (s.entries - 1);
@@ -738,14 +734,14 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
     if (fixed && inst > 1) {
       const unsigned grid = (unsigned)std::min<size_t>(s.lvl_blocks[0], queue_grid<F>());
       k_msm_accum0_queue<F, true><<<grid, seg_threads<F>(), 0, st>>>(
-          L.skey, L.sval, total_p, ps, s.k0, L.buckets, ok, L.ppt[1],
+          L.srec, total_p, ps, s.k0, L.buckets, ok, L.ppt[1],
           (uint32_t)s.lvl_blocks[0], L.tileq);
     } else if (fixed)
       k_msm_accum0<F, true><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
-          L.skey, L.sval, total_p, ps, s.k0, L.buckets, ok, L.ppt[1]);
+          L.srec, total_p, ps, s.k0, L.buckets, ok, L.ppt[1]);
     else
       k_msm_accum0<F, false><<<(unsigned)s.lvl_blocks[0], seg_threads<F>(), 0, st>>>(
-          L.skey, L.sval, total_p, ps, s.k0, L.buckets, ok, L.ppt[1]);
+          L.srec, total_p, ps, s.k0, L.buckets, ok, L.ppt[1]);
     ZK_LAUNCHED();
   }
   for (int l = 1; l < s.levels; l++) {
