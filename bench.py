@@ -50,6 +50,10 @@ UNIT = "proofs/s"
 # carry-chain probe counted this way can exceed the issued one.
 FP_MULTS_PER_POINT = {"accum_g1": 176.0, "accum_g2": 528.0}
 IMAD_PER_FP_MULT = 264.0
+# what the fixed-base accumulation issues per sorted record (one mixed XYZZ
+# add): G1 8 products x 232 + one shared-reduction difference of products
+# (2 x 96 + 136); G2 8 Fp2 products x 560 + 2 Fp2 squares x 2 x 232
+ISSUED_IMAD_PER_RECORD = {"accum_g1": 8 * 232 + 2 * 96 + 136, "accum_g2": 8 * 560 + 2 * 2 * 232}
 
 
 def parse_args():
@@ -264,9 +268,12 @@ def traffic_per_point():
     return out
 
 
-def roofline_of(kind, rec, peak, step_ms):
+def roofline_of(kind, rec, peak, step_ms, records_per_point=None):
     """Algorithmic IMAD-class ops of the accumulation kernels of `kind` over
-    their measured event time, against the measured IMAD peak."""
+    their measured event time, against the measured IMAD peak.  With the
+    fixed-base window count, `issued` repeats it with the ops the kernel
+    actually issues per sorted record (fewer records and cheaper products
+    than the convention counts)."""
     kms, kl, ku = rec
     if not kl or kms <= 0:
         return None
@@ -279,7 +286,27 @@ def roofline_of(kind, rec, peak, step_ms):
          "avg_launch_ms": kms / kl, "launches": int(kl)}
     if step_ms:
         r["share_of_step"] = kms / step_ms
+    if records_per_point:
+        ia = ku * records_per_point * ISSUED_IMAD_PER_RECORD[kind] / (kms / 1e3) / 1e12
+        r["issued"] = {"records_per_point": records_per_point,
+                       "imad_per_record": ISSUED_IMAD_PER_RECORD[kind],
+                       "achieved": ia, "frac": ia / peak}
     return r
+
+
+def table_windows(args, tuned, group):
+    """Windows (records per point) of the fixed-base tables the resident
+    proof uses: --table-c, else the tuned window bits, else the default."""
+    from zyklop_b200.api import table_c_default
+    c = int(args.table_c.split(",")[group - 1])
+    if c <= 0 and isinstance(tuned, list):
+        for t in tuned:
+            f = t.split()
+            if len(f) == 5 and f[0] == "table" and f[1] == str(group) and f[2] == str(args.log_domain):
+                c = int(f[4])
+    if c <= 0:
+        c = table_c_default(args.log_domain)
+    return 254 // c + 1
 
 
 def run_mine(args, dist):
@@ -347,7 +374,8 @@ def run_mine(args, dist):
     # time shared with the other streams)
     kinds = {k: (prof.ms[i], prof.launches[i], prof.units[i]) for i, k in enumerate(Profile.KINDS)}
     dom = max(FP_MULTS_PER_POINT, key=lambda k: kinds[k][0])
-    roofline = roofline_of(dom, kinds[dom], peak.value, ms)
+    wins = {"accum_g1": table_windows(args, tuned, 1), "accum_g2": table_windows(args, tuned, 2)}
+    roofline = roofline_of(dom, kinds[dom], peak.value, ms, wins[dom])
     other = {k: {"ms_per_step": v[0] / args.steps, "launches": int(v[1])} for k, v in kinds.items()}
 
     # the same kernels with a proof's MSMs back to back on one stream (an
@@ -365,7 +393,8 @@ def run_mine(args, dist):
     check(L.zk_ctx_set_prove_streams(ctx, 0))
     assert np.array_equal(proof, reference_proof), "proofs changed with one MSM stream"
     skinds = {k: (prof.ms[i], prof.launches[i], prof.units[i]) for i, k in enumerate(Profile.KINDS)}
-    roofline_serial = {k: roofline_of(k, skinds[k], peak.value, None) for k in FP_MULTS_PER_POINT}
+    roofline_serial = {k: roofline_of(k, skinds[k], peak.value, None, wins[k])
+                       for k in FP_MULTS_PER_POINT}
 
     # e2e through the one-shot host-buffer entry point
     e2e_steps = args.e2e_steps or min(args.steps, 5)
