@@ -374,7 +374,10 @@ def run_mine(args, dist):
     # time shared with the other streams)
     kinds = {k: (prof.ms[i], prof.launches[i], prof.units[i]) for i, k in enumerate(Profile.KINDS)}
     dom = max(FP_MULTS_PER_POINT, key=lambda k: kinds[k][0])
-    wins = {"accum_g1": table_windows(args, tuned, 1), "accum_g2": table_windows(args, tuned, 2)}
+    # issued work assumes every window of every point makes a record: true for
+    # uniform scalars, not for circom-like witnesses (zero digits are skipped)
+    wins = ({"accum_g1": table_windows(args, tuned, 1), "accum_g2": table_windows(args, tuned, 2)}
+            if args.witness == "uniform" else {"accum_g1": None, "accum_g2": None})
     roofline = roofline_of(dom, kinds[dom], peak.value, ms, wins[dom])
     other = {k: {"ms_per_step": v[0] / args.steps, "launches": int(v[1])} for k, v in kinds.items()}
 
