@@ -427,12 +427,11 @@ __device__ __forceinline__ void accum0_tile(size_t b, SegNode<F>* sm,
   seg_block_finish(sm, key_before, key_after, buckets, okey, opt, b);
 }
 
-// One tile per block.  Four blocks per SM: the G1 form needs 136 registers
-// unbounded (three blocks); capped at 128 it spills ~160 B a thread and is
-// still ~1-2 % faster (G1 MSM 2^22 18.1 -> 17.8 ms).  The G2 form is at the
-// 255-register limit either way.
+// One tile per block.  The G1 form takes 148 registers (three blocks per
+// SM); capping it at 128 for four blocks spilled ~450 B a thread and ran
+// ~1 % slower.  The G2 form is at the 255-register limit either way.
 template <class F, bool kFixed>
-__global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0(
+__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0(
     const uint2* __restrict__ srec, const uint32_t* __restrict__ total_p,
     const __grid_constant__ PointSrc<F> src, int K,
     xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt) {
@@ -443,10 +442,11 @@ __global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0(
 // Persistent form for multi-instance chains (several proofs' MSMs): a grid
 // of as many blocks as the device holds at once, each claiming record tiles
 // (instance, bucket range) from a device work queue until all `ntiles` are
-// taken.  `queue` starts at zero.  Four blocks per SM, like the one-tile
-// form.
+// taken.  `queue` starts at zero.  Uncapped like the one-tile form (156
+// registers, three G1 blocks per SM): fused batches ran ~2 % faster than
+// with a 128-register cap.
 template <class F, bool kFixed>
-__global__ void __launch_bounds__(seg_threads<F>(), 4) k_msm_accum0_queue(
+__global__ void __launch_bounds__(seg_threads<F>()) k_msm_accum0_queue(
     const uint2* __restrict__ srec, const uint32_t* __restrict__ total_p,
     const __grid_constant__ PointSrc<F> src, int K,
     xyzz<F>* __restrict__ buckets, uint32_t* __restrict__ okey, xyzz<F>* __restrict__ opt,
