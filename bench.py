@@ -51,9 +51,11 @@ UNIT = "proofs/s"
 FP_MULTS_PER_POINT = {"accum_g1": 176.0, "accum_g2": 528.0}
 IMAD_PER_FP_MULT = 264.0
 # what the fixed-base accumulation issues per sorted record (one mixed XYZZ
-# add): G1 8 products x 232 + one shared-reduction difference of products
-# (2 x 96 + 136); G2 8 Fp2 products x 560 + 2 Fp2 squares x 2 x 232
-ISSUED_IMAD_PER_RECORD = {"accum_g1": 8 * 232 + 2 * 96 + 136, "accum_g2": 8 * 560 + 2 * 2 * 232}
+# add): G1 6 products x 232 + 2 squares x (72 + 136) + one shared-reduction
+# difference of products (2 x 96 + 136); G2 8 Fp2 products x 560 + 2 Fp2
+# squares x 2 x 232
+ISSUED_IMAD_PER_RECORD = {"accum_g1": 6 * 232 + 2 * (72 + 136) + 2 * 96 + 136,
+                          "accum_g2": 8 * 560 + 2 * 2 * 232}
 
 
 def parse_args():
