@@ -56,7 +56,7 @@ Shape make_shape(size_t n, bool g2, const MsmConfig& cfg, bool fixed = false, in
   s.records = std::max<size_t>((size_t)s.W * n, 1);
   s.k0 = cfg.k0 > 0 ? cfg.k0 : msm_default_k0(n, fixed);
   s.k1 = cfg.k1;
-  s.chunk = cfg.chunk > 0 ? cfg.chunk : msm_default_chunk(n);
+  s.chunk = cfg.chunk > 0 ? cfg.chunk : msm_default_chunk(n, fixed, s.c);
   s.J = (s.B + s.chunk - 1) / s.chunk;
   size_t rec = s.records;
   int per_thread = s.k0;
@@ -788,10 +788,14 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
 // window bits lg - 4 up to 2^16 points, then lg - 3 capped at 16 through
 // 2^22 (a window's 2^15 buckets of XYZZ sums stay L2-resident), growing
 // again by one per doubling beyond 2^22; records per accumulation thread 16
-// up to 2^15 points, 32 up to 2^17, then 64 (fixed-base) or
-// 128 / 256 (windowed, below / from 2^22); buckets per reduction thread 4
-// up to 2^16 points, 8 up to 2^18, then 16.  Small MSMs are bound by the
-// depth of their dependent additions, so they get short per-thread runs.
+// up to 2^15 points, 32 up to 2^17, then 64 / 128 (fixed-base, below / from
+// 2^20) or 128 / 256 (windowed, below / from 2^22); buckets per reduction
+// thread 4 up to 2^16 points, 8 up to 2^18, then 16.  Small MSMs are bound
+// by the depth of their dependent additions, so they get short per-thread
+// runs.  Fixed-base sets of 2^19 or more buckets (windows of 20 bits and
+// up) take 32 buckets per reduction thread: timed as whole 2^20 proofs,
+// where four MSMs overlap, k0 128 / chunk 32 ran 23.3 ms against 24.8 ms
+// for 64 / 16 (less reduction work beats a shorter chain there).
 int msm_default_c(size_t n, bool g2) {
   (void)g2;
   int lg = 0;
@@ -807,11 +811,12 @@ int msm_default_k0(size_t n, bool fixed) {
   while ((size_t(1) << lg) < n) lg++;
   if (lg <= 15) return 16;
   if (lg <= 17) return 32;
-  if (fixed) return 64;
+  if (fixed) return lg <= 19 ? 64 : 128;
   return lg < 22 ? 128 : 256;
 }
 
-int msm_default_chunk(size_t n) {
+int msm_default_chunk(size_t n, bool fixed, int c) {
+  if (fixed && c >= 20) return 32;
   int lg = 0;
   while ((size_t(1) << lg) < n) lg++;
   return lg <= 16 ? 4 : (lg <= 18 ? 8 : 16);

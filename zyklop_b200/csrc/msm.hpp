@@ -69,7 +69,7 @@ struct MsmResult {
 
 int msm_default_c(size_t n, bool g2);
 int msm_default_k0(size_t n, bool fixed);
-int msm_default_chunk(size_t n);
+int msm_default_chunk(size_t n, bool fixed = false, int c = 0);
 
 // Device scratch bytes one MSM of n points needs with this configuration.
 size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg);

@@ -163,12 +163,13 @@ struct Search {
   int reps;
   Search(zk_ctx* x, const Inputs& i, int f, const void* t, int r)
       : ctx(x), in(i), fixed_c(f), table(t), reps(r) {}
-  void trial(const MsmConfig& cfg) {
+  // `margin`: the fraction by which a candidate must beat the best so far
+  void trial(const MsmConfig& cfg, double margin = 0) {
     std::vector<uint64_t> got;
     const double ms = time_msm(ctx, in, cfg, fixed_c, table, scratch, reps, got);
     if (expect.empty()) expect = got;
     ZK_REQUIRE(got == expect, ZK_EINTERNAL, "autotune: MSM settings disagree on the result");
-    if (ms < best_ms) {
+    if (ms < best_ms * (1 - margin)) {
       best_ms = ms;
       best = cfg;
     }
@@ -199,6 +200,15 @@ TuneResult autotune_msm(zk_ctx* ctx, int group, int log_n, int dist, int fixed_c
   MsmConfig cfg = ctx->msm_cfg[g2 ? 1 : 0];
   cfg.k0 = 64;
   cfg.chunk = 16;
+  // Fixed-base MSMs start from the size defaults, which come from timing
+  // whole proofs (overlapping MSMs), and leave them only for a clear win:
+  // a lone MSM favours shorter dependency chains and its timing is noisy.
+  double margin = 0;
+  if (fixed_c) {
+    cfg.k0 = msm_default_k0(n, true);
+    cfg.chunk = msm_default_chunk(n, true, fixed_c);
+    margin = 0.02;
+  }
   if (!fixed_c) {
     // window bits first (the dominant choice), then the split threshold and
     // the reduction chunk at the best window
@@ -211,15 +221,17 @@ TuneResult autotune_msm(zk_ctx* ctx, int group, int log_n, int dist, int fixed_c
     cfg.c = fixed_c;
     s.trial(cfg);
   }
-  for (int k0 : {16, 32, 128, 256}) {
+  for (int k0 : {16, 32, 64, 128, 256}) {
+    if (k0 == s.best.k0) continue;
     MsmConfig k = s.best;
     k.k0 = k0;
-    s.trial(k);
+    s.trial(k, margin);
   }
-  for (int chunk : {4, 8, 32, 64}) {
+  for (int chunk : {4, 8, 16, 32, 64}) {
+    if (chunk == s.best.chunk) continue;
     MsmConfig k = s.best;
     k.chunk = chunk;
-    s.trial(k);
+    s.trial(k, margin);
   }
   MsmConfig rec = s.best;
   if (fixed_c) rec.c = 0;  // fixed-base MSMs take c from their table
