@@ -28,6 +28,8 @@ struct ProveWs {
   cudaStream_t st[kStreams] = {};
   cudaEvent_t ev_we = nullptr, ev_begin = nullptr, ev_all = nullptr;
   cudaEvent_t ev_done[kStreams] = {};
+  cudaEvent_t ev_merge = nullptr;  // C's buckets accumulated (H reduces them with its own)
+  MsmMerge merge_c;
   DeviceBuffer we, aw, bw, cw, h;
   DeviceBuffer msm[kStreams];
   PinnedBuffer win[kStreams];

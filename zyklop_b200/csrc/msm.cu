@@ -500,6 +500,17 @@ __global__ void __launch_bounds__(seg_threads<F>()) k_msm_accumN(
   seg_block_finish(sm, key_before, key_after, buckets, okey, opt, (size_t)blockIdx.x);
 }
 
+// dst[i] += src[i]: the buckets of two MSMs whose results are added, so one
+// reduction yields the sum.
+template <class F>
+__global__ void __launch_bounds__(128) k_msm_bucket_add(xyzz<F>* __restrict__ dst,
+                                                        const xyzz<F>* __restrict__ src,
+                                                        size_t count) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  st_pod(&dst[i], xyzz_add(ld_pod(&dst[i]), ld_pod(&src[i])));
+}
+
 // ------------------------------------------------------ bucket reduction
 // Window sums sum_b (b+1) S_b, without per-chunk scalar multiplications and
 // without long serial chains above the first level.
@@ -694,7 +705,8 @@ int queue_grid() {
 template <class F>
 MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size_t n_max,
                       size_t n_total, void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
-                      cudaStream_t st, bool fixed) {
+                      cudaStream_t st, bool fixed, MsmMerge* merge_out = nullptr,
+                      const MsmMerge* merge_in = nullptr) {
   constexpr bool g2 = sizeof(F) == 64;
   ZK_REQUIRE(n_max < (size_t(1) << 31), ZK_EINVAL, "msm: too many points (max 2^31 - 1)");
   ZK_REQUIRE(inst >= 1 && inst <= kMaxInst, ZK_EINVAL, "msm: 1..64 instances per launch");
@@ -749,6 +761,28 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
     uint32_t* ok = (l + 1 < s.levels) ? L.pkey[out] : nullptr;
     k_msm_accumN<F><<<(unsigned)s.lvl_blocks[l], seg_threads<F>(), 0, st>>>(
         L.pkey[in], L.ppt[in], s.lvl_records[l], s.lvl_k[l], L.buckets, ok, L.ppt[out]);
+    ZK_LAUNCHED();
+  }
+  const size_t nbuckets = (size_t)s.Wk * s.B;
+  if (merge_out && inst == 1) {
+    // producer: the consumer reduces these buckets together with its own
+    merge_out->buckets = L.buckets;
+    merge_out->count = nbuckets;
+    merge_out->c = s.c;
+    merge_out->fixed = fixed;
+    merge_out->g2 = g2;
+    if (merge_out->ready) ZK_CUDA(cudaEventRecord(merge_out->ready, st));
+    MsmResult none;
+    none.c = s.c;
+    return none;
+  }
+  if (merge_in && merge_in->buckets) {
+    ZK_REQUIRE(inst == 1 && merge_in->count == nbuckets && merge_in->c == s.c &&
+                   merge_in->fixed == fixed && merge_in->g2 == g2,
+               ZK_EINTERNAL, "msm: merged bucket sets differ in shape");
+    ZK_CUDA(cudaStreamWaitEvent(st, merge_in->ready, 0));
+    k_msm_bucket_add<F><<<(unsigned)((nbuckets + 127) / 128), 128, 0, st>>>(
+        L.buckets, static_cast<const xyzz<F>*>(merge_in->buckets), nbuckets);
     ZK_LAUNCHED();
   }
   int log_span = 0;
@@ -806,6 +840,10 @@ int msm_default_c(size_t n, bool g2) {
   return c;
 }
 
+int msm_effective_c(size_t n, bool g2, const MsmConfig& cfg) {
+  return cfg.c > 0 ? cfg.c : msm_default_c(n, g2);
+}
+
 int msm_default_k0(size_t n, bool fixed) {
   int lg = 0;
   while ((size_t(1) << lg) < n) lg++;
@@ -860,7 +898,8 @@ namespace {
 template <class F>
 MsmResult enqueue_fixed_multi(int inst, const void* const* tables, const uint64_t* const* scalars,
                               const size_t* n, int c, void* scratch, size_t bytes,
-                              const MsmConfig& cfg, cudaStream_t st) {
+                              const MsmConfig& cfg, cudaStream_t st, MsmMerge* merge_out = nullptr,
+                              const MsmMerge* merge_in = nullptr) {
   ZK_REQUIRE(inst >= 1 && inst <= kMaxInst, ZK_EINVAL, "msm: 1..64 instances per launch");
   MsmConfig k = cfg;
   k.c = c;
@@ -876,12 +915,14 @@ MsmResult enqueue_fixed_multi(int inst, const void* const* tables, const uint64_
     n_max = std::max(n_max, n[i]);
     n_total += n[i];
   }
-  return msm_enqueue<F>(ss, ps, inst, n_max, n_total, scratch, bytes, k, st, true);
+  return msm_enqueue<F>(ss, ps, inst, n_max, n_total, scratch, bytes, k, st, true, merge_out,
+                       merge_in);
 }
 
 template <class F>
 MsmResult enqueue_windowed(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                           size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
+                           size_t bytes, const MsmConfig& cfg, cudaStream_t st,
+                           MsmMerge* merge_out = nullptr, const MsmMerge* merge_in = nullptr) {
   ScalarSrc ss{};
   ss.sc[0] = scalars;
   ss.n[0] = (uint32_t)std::min(n, size_t(0xffffffffu));
@@ -889,13 +930,18 @@ MsmResult enqueue_windowed(const PointsView& pts, const uint64_t* scalars, size_
   ps.x = reinterpret_cast<const F*>(pts.x);
   ps.y = reinterpret_cast<const F*>(pts.y);
   ps.stride = pts.stride;
-  return msm_enqueue<F>(ss, ps, 1, n, n, scratch, bytes, cfg, st, false);
+  return msm_enqueue<F>(ss, ps, 1, n, n, scratch, bytes, cfg, st, false, merge_out, merge_in);
 }
 }  // namespace
 
 MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
-                            void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
-  return msm_enqueue_fixed_multi(g2, 1, &table, &scalars, &n, c, scratch, bytes, cfg, st);
+                            void* scratch, size_t bytes, const MsmConfig& cfg, cudaStream_t st,
+                            MsmMerge* merge_out, const MsmMerge* merge_in) {
+  if (g2)
+    return enqueue_fixed_multi<fp2_t>(1, &table, &scalars, &n, c, scratch, bytes, cfg, st,
+                                      merge_out, merge_in);
+  return enqueue_fixed_multi<fp_t>(1, &table, &scalars, &n, c, scratch, bytes, cfg, st, merge_out,
+                                   merge_in);
 }
 
 MsmResult msm_enqueue_fixed_multi(bool g2, int inst, const void* const* tables,
@@ -907,8 +953,9 @@ MsmResult msm_enqueue_fixed_multi(bool g2, int inst, const void* const* tables,
 }
 
 MsmResult msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                         size_t bytes, const MsmConfig& cfg, cudaStream_t st) {
-  return enqueue_windowed<fp_t>(pts, scalars, n, scratch, bytes, cfg, st);
+                         size_t bytes, const MsmConfig& cfg, cudaStream_t st, MsmMerge* merge_out,
+                         const MsmMerge* merge_in) {
+  return enqueue_windowed<fp_t>(pts, scalars, n, scratch, bytes, cfg, st, merge_out, merge_in);
 }
 MsmResult msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
                          size_t bytes, const MsmConfig& cfg, cudaStream_t st) {

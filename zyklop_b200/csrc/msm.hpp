@@ -67,7 +67,26 @@ struct MsmResult {
   int log_span = 0;
 };
 
+// Two MSMs whose results are added (a proof's C and H parts of pi_C) can
+// share one bucket reduction.  The producer (`merge_out`) stops after its
+// bucket accumulation and leaves its buckets, returning an empty result
+// (zero windows: the point at infinity).  The consumer (`merge_in`, same
+// kind, window bits and bucket count) adds those buckets into its own
+// before its reduction, so its result is the sum of both MSMs.  `ready`
+// (the caller's event) is recorded after the producer's accumulation; the
+// producer's scratch must stay untouched until the consumer has run.
+struct MsmMerge {
+  const void* buckets = nullptr;
+  size_t count = 0;
+  int c = 0;
+  bool fixed = false;
+  bool g2 = false;
+  cudaEvent_t ready = nullptr;
+};
+
 int msm_default_c(size_t n, bool g2);
+// Window bits a windowed MSM of n points runs with under cfg.
+int msm_effective_c(size_t n, bool g2, const MsmConfig& cfg);
 int msm_default_k0(size_t n, bool fixed);
 int msm_default_chunk(size_t n, bool fixed = false, int c = 0);
 
@@ -76,8 +95,10 @@ size_t msm_scratch_bytes(size_t n, bool g2, const MsmConfig& cfg);
 
 // Enqueue the GPU part of an MSM on `stream`; its result stays inside
 // `scratch` (which must hold msm_scratch_bytes(n, ...) bytes) until copied.
+// `merge_out` / `merge_in`: see MsmMerge.
 MsmResult msm_g1_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
-                         size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream);
+                         size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream,
+                         MsmMerge* merge_out = nullptr, const MsmMerge* merge_in = nullptr);
 MsmResult msm_g2_enqueue(const PointsView& pts, const uint64_t* scalars, size_t n, void* scratch,
                          size_t scratch_bytes, const MsmConfig& cfg, cudaStream_t stream);
 
@@ -93,7 +114,8 @@ void msm_precompute(bool g2, const PointsView& pts, size_t n, int c, void* table
                     cudaStream_t stream);
 MsmResult msm_enqueue_fixed(bool g2, const void* table, const uint64_t* scalars, size_t n, int c,
                             void* scratch, size_t scratch_bytes, const MsmConfig& cfg,
-                            cudaStream_t stream);
+                            cudaStream_t stream, MsmMerge* merge_out = nullptr,
+                            const MsmMerge* merge_in = nullptr);
 // Several fixed-base MSMs with the same window bits in one launch chain: one
 // instance per (table, scalars, n); their records share the sort, the
 // load-balanced accumulation and the bucket reduction (instance i's buckets

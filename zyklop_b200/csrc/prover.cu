@@ -124,6 +124,7 @@ void ProveWs::init() {
   }
   ZK_CUDA(cudaEventCreateWithFlags(&ev_we, cudaEventDisableTiming));
   ZK_CUDA(cudaEventCreateWithFlags(&ev_begin, cudaEventDisableTiming));
+  ZK_CUDA(cudaEventCreateWithFlags(&ev_merge, cudaEventDisableTiming));
   ready = true;
 }
 
@@ -135,6 +136,7 @@ ProveWs::~ProveWs() {
     cudaEventDestroy(ev_done[i]);
   }
   cudaEventDestroy(ev_we);
+  cudaEventDestroy(ev_merge);
   cudaEventDestroy(ev_begin);
   cudaEventDestroy(ev_all);
   drop_graph();
@@ -376,26 +378,38 @@ void ws_stage(zk_circuit* c, ProveWs& ws, const uint64_t* witness, bool on_devic
 
 // MSM i of a proof (indexed like ProveWs::msm) on stream i mod nstreams,
 // after the staged witness; its window sums land in ws.win[i] and
-// ev_done[i] marks them.
+// ev_done[i] marks them.  `mo` / `mi`: the C and H MSMs share one bucket
+// reduction (msm.hpp, MsmMerge); C's own result is then empty.
 void ws_msm(zk_circuit* c, ProveWs& ws, int i, bool g2, const DeviceBuffer& pts,
-            const DeviceBuffer& tab, const uint64_t* sc, size_t cnt) {
+            const DeviceBuffer& tab, const uint64_t* sc, size_t cnt, MsmMerge* mo = nullptr,
+            const MsmMerge* mi = nullptr) {
   const bool fixed = c->tab_c[0] != 0;
   const int si = i % ws.nstreams;
   cudaStream_t st = ws.st[si];
   if (si) ZK_CUDA(cudaStreamWaitEvent(st, ws.ev_we, 0));
   if (fixed)
     ws.res[i] = msm_enqueue_fixed(g2, tab.ptr, sc, cnt, c->tab_c[g2 ? 1 : 0], ws.msm[i].ptr,
-                                  ws.msm[i].cap, ws.cfg[i], st);
+                                  ws.msm[i].cap, ws.cfg[i], st, mo, mi);
   else if (g2)
     ws.res[i] = msm_g2_enqueue(points_aos(pts.ptr, true), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap,
                                ws.cfg[i], st);
   else
     ws.res[i] = msm_g1_enqueue(points_aos(pts.ptr, false), sc, cnt, ws.msm[i].ptr, ws.msm[i].cap,
-                               ws.cfg[i], st);
+                               ws.cfg[i], st, mo, mi);
   ZK_REQUIRE(ws.res[i].bytes <= kMaxWindowBytes, ZK_EINTERNAL, "prove: MSM result too large");
-  ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, ws.res[i].d_data, ws.res[i].bytes, cudaMemcpyDeviceToHost,
-                          st));
+  if (ws.res[i].bytes)
+    ZK_CUDA(cudaMemcpyAsync(ws.win[i].ptr, ws.res[i].d_data, ws.res[i].bytes,
+                            cudaMemcpyDeviceToHost, st));
   ZK_CUDA(cudaEventRecord(ws.ev_done[i], st));
+}
+
+// Whether the C MSM (index 3) and the H MSM (index 0) of a proof can share
+// one bucket reduction: pi_C adds their results, so they can when both run
+// with the same window bits (fixed-base: always, one G1 table size).
+bool ws_merge_ch(const zk_circuit* c, const ProveWs& ws) {
+  if (c->tab_c[0] != 0) return true;
+  const size_t nc = c->m1 - c->l - 1;
+  return msm_effective_c(nc, false, ws.cfg[3]) == msm_effective_c(c->n, false, ws.cfg[0]);
 }
 
 // The device part of a proof, from the staged witness to the MSM results in
@@ -410,9 +424,15 @@ void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg
   ZK_CUDA(cudaEventRecord(ws.ev_we, s0));
   auto launch = [&](int i, bool g2, const DeviceBuffer& pts, const DeviceBuffer& tab,
                     const uint64_t* sc, size_t cnt) { ws_msm(c, ws, i, g2, pts, tab, sc, cnt); };
+  // C leaves its buckets to H's reduction unless intermediates want each
+  // MSM's own result
+  const bool merge = !dbg && ws_merge_ch(c, ws);
+  ws.merge_c = MsmMerge{};
+  ws.merge_c.ready = ws.ev_merge;
   launch(1, false, c->pts_a, c->tab_a, we, m1 + 1);
   launch(2, true, c->pts_b2, c->tab_b2, we, m1 + 1);
-  launch(3, false, c->pts_c, c->tab_c_pts, we + 4 * (l + 2), nc);
+  ws_msm(c, ws, 3, false, c->pts_c, c->tab_c_pts, we + 4 * (l + 2), nc,
+         merge ? &ws.merge_c : nullptr);
   if (blind) launch(4, false, c->pts_b1, c->tab_b1, we, m1 + 1);
 
   spmv_enqueue(c, we, ws.aw.as<uint64_t>(), ws.bw.as<uint64_t>(), s0);
@@ -423,7 +443,8 @@ void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg
   hpoly(ctx->ntt, ws.aw.as<uint64_t>(), ws.bw.as<uint64_t>(), ws.cw.as<uint64_t>(), c->log_n,
         ws.h.as<uint64_t>(), s0);
   if (dbg && dbg->h) ZK_CUDA(cudaMemcpyAsync(dbg->h, ws.h.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
-  launch(0, false, c->pts_h, c->tab_h, ws.h.as<uint64_t>(), n);
+  ws_msm(c, ws, 0, false, c->pts_h, c->tab_h, ws.h.as<uint64_t>(), n, nullptr,
+         merge ? &ws.merge_c : nullptr);
   for (int i = 1; i < (blind ? 5 : 4); i++) ZK_CUDA(cudaStreamWaitEvent(s0, ws.ev_done[i], 0));
 }
 
@@ -638,7 +659,10 @@ void prove_oneshot(zk_ctx* ctx, const BinFile& zkey, const uint64_t* witness, si
   upload_points(c, z, kSetA, ws.st[1 % ws.nstreams], sg);
   ws_msm(c, ws, 1, false, c->pts_a, none, we, m1 + 1);
   upload_points(c, z, kSetC, ws.st[3 % ws.nstreams], sg);
-  ws_msm(c, ws, 3, false, c->pts_c, none, we + 4 * (l + 2), nc);
+  const bool merge = ws_merge_ch(c, ws);
+  ws.merge_c = MsmMerge{};
+  ws.merge_c.ready = ws.ev_merge;
+  ws_msm(c, ws, 3, false, c->pts_c, none, we + 4 * (l + 2), nc, merge ? &ws.merge_c : nullptr);
   // section 4 -> CSR -> A.w, B.w -> h on stream 0, the H points beside it
   CsrScratch csr;
   uint32_t* h_bad = ws.flag.as<uint32_t>();
@@ -650,7 +674,8 @@ void prove_oneshot(zk_ctx* ctx, const BinFile& zkey, const uint64_t* witness, si
   upload_points(c, z, kSetH, sh, sg);
   ZK_CUDA(cudaEventRecord(ws.ev_done[4], sh));
   ZK_CUDA(cudaStreamWaitEvent(s0, ws.ev_done[4], 0));
-  ws_msm(c, ws, 0, false, c->pts_h, none, ws.h.as<uint64_t>(), n);
+  ws_msm(c, ws, 0, false, c->pts_h, none, ws.h.as<uint64_t>(), n, nullptr,
+         merge ? &ws.merge_c : nullptr);
   for (int i = 1; i < 4; i++) ZK_CUDA(cudaStreamWaitEvent(s0, ws.ev_done[i], 0));
   ZK_CUDA(cudaEventRecord(ws.ev_all, s0));
   ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_all, 0));
