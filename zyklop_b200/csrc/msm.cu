@@ -776,7 +776,8 @@ MsmResult msm_enqueue(const ScalarSrc& ss, const PointSrc<F>& ps, int inst, size
     none.c = s.c;
     return none;
   }
-  if (merge_in && merge_in->buckets) {
+  if (merge_in) {
+    ZK_REQUIRE(merge_in->buckets, ZK_EINTERNAL, "msm: merged MSM left no buckets");
     ZK_REQUIRE(inst == 1 && merge_in->count == nbuckets && merge_in->c == s.c &&
                    merge_in->fixed == fixed && merge_in->g2 == g2,
                ZK_EINTERNAL, "msm: merged bucket sets differ in shape");
