@@ -190,8 +190,8 @@ int zk_circuit_info(const zk_circuit* c, uint32_t* n_vars, uint32_t* n_public, u
  * one shared bucket set: one bucket reduction per MSM instead of one per
  * window and no doubling chain, with larger windows (fewer additions).
  * c_g1 / c_g2: window bits (0 = default for the size).  Proofs are
- * unchanged bit for bit.  The CRS-residency format of SURVEY 8(f) row 2;
- * the reference has no counterpart. */
+ * unchanged bit for bit.  A resident-CRS format for repeated proofs of one
+ * circuit; the reference has no counterpart. */
 int zk_circuit_precompute(zk_circuit* c, int c_g1, int c_g2);
 
 /* Proves with a witness of n_witness >= nVars canonical Fr values (wtns
