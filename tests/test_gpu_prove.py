@@ -532,3 +532,28 @@ def test_fused_group_at_the_instance_limit(api, files):
     finally:
         api.set_batch_mode(api.BATCH_AUTO, 16)
     c.close()
+
+
+@pytest.mark.parametrize("c_c,c_h", [(8, 8), (7, 8)])
+def test_c_and_h_msms_share_a_reduction_only_with_equal_windows(api, oracle, files, c_c, c_h):
+    """pi_C adds the C and H MSMs, so a proof lets C's buckets go into H's
+    reduction when both run with the same window bits.  The C MSM takes the
+    witness's (circom-like: skewed) tuned settings and H the uniform ones;
+    importing different window bits for the two must turn the sharing off.
+    Proofs stay exact either way, one-shot and resident (windowed)."""
+    from zyklop_b200._lib import check, lib
+    L = lib()
+    z, w = files["c10"]
+    want = oracle.prove(blob(z), blob(w))
+    ctx = ctypes.c_void_p()
+    check(L.zk_ctx_create(0, ctypes.byref(ctx)))
+    try:
+        api.tune_import(f"msm 1 10 1 0 {c_c} 16 16 4\nmsm 1 10 0 0 {c_h} 16 16 4\n", ctx=ctx)
+        assert np.array_equal(api.prove_files(z, w, ctx=ctx), want)
+        c = api.Circuit(z, ctx=ctx)
+        wit = api.read_wtns(w)
+        assert np.array_equal(c.prove(wit), want)
+        assert np.array_equal(c.prove(wit), want)
+        c.close()
+    finally:
+        check(L.zk_ctx_destroy(ctx))
