@@ -162,8 +162,8 @@ int zk_msm_table_free(zk_msm_table* t);
 
 /* Pippenger parameters for subsequent MSMs on this context (group 1 or 2):
  * window bits c (0 = automatic), records per thread k0 (0 = by size) / k1,
- * and the fan-in `chunk` (a power of two, 0 = by size) of the first
- * bucket-reduction level.
+ * and the fan-in `chunk` (a power of two, 0 = by size, and for fixed-base
+ * MSMs by window bits) of the first bucket-reduction level.
  * Replaces the reference's compile-time
  * MSM_G1_C_BITS / C_BITS and ZK_G1_* / ZK_G2_* environment knobs
  * (include/msm_g1.cuh:45-117, include/msm_g2.cuh:39-116). */
