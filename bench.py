@@ -19,8 +19,13 @@ inputs, uniform witness), produced by libzyklop_b200.so.
 
 --impl reference runs the reference's own sm_100a build (oracle/_ref,
 compiled from the reference sources) through its groth16Prove on the same
-files.  With torchrun, every rank proves independently (replicas; the prover
-is single-GPU by design).
+files, and the same primitive sweep through its msm_g1 / msm_g2_device / ntt /
+computeHPoly; it writes its proofs and primitive results to the work
+directory, and this arm checks its own against them bit for bit
+(parity_vs_reference).  All inputs are written by zyklop_b200/bin/zk_synth in
+a child process, so the reference process never loads this library.  With
+torchrun, every rank proves independently (replicas; the prover is
+single-GPU by design).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--log-domain L]
 """
@@ -84,6 +89,12 @@ def parse_args():
     p.add_argument("--prim-g1", default="18,20,22,24", help="G1 MSM sizes (log2); empty skips")
     p.add_argument("--prim-g2", default="18,20")
     p.add_argument("--prim-ntt", default="16,18,20,22,24")
+    p.add_argument("--prim-hpoly", default="16,20,22", help="H pipeline (coset INTT/NTT) sizes")
+    p.add_argument("--config2-log", type=int, default=22,
+                   help="single proof, circom-like witness, 1-4 nonzeros per row; 0 skips")
+    p.add_argument("--config2-steps", type=int, default=10)
+    p.add_argument("--parity-only", action="store_true",
+                   help="(--impl reference) write the reference outputs without timing")
     return p.parse_args()
 
 
@@ -196,6 +207,17 @@ def silenced():
 
 
 # ------------------------------------------------------------- workload
+SYNTH = os.path.join(ROOT, "zyklop_b200", "bin", "zk_synth")
+
+
+def run_synth(*argv):
+    """zk_synth in a child process (this process never loads the library for
+    input generation, so the reference arm maps only the reference build)."""
+    r = subprocess.run([SYNTH, *[str(a) for a in argv]], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"zk_synth {' '.join(map(str, argv))} failed: {r.stderr.strip()}")
+
+
 def synth_cached(args, dist, lg, witness, seed):
     """Seeded synthetic circuit + witness files, generated once per workdir.
     uniform: 2 nonzeros per A/B row; circom: 1-4 nonzeros per row and the
@@ -206,10 +228,7 @@ def synth_cached(args, dist, lg, witness, seed):
     done = os.path.join(d, "ok")
     if dist.rank == 0 and not os.path.exists(done):
         os.makedirs(d, exist_ok=True)
-        from zyklop_b200 import api
-        nnz = (2, 2) if witness == "uniform" else (1, 4)
-        api.synth_circuit(z, w, lg, n_public=8, n_private_inputs=8, nnz=nnz,
-                          witness=witness, seed=seed)
+        run_synth("circuit", z, w, lg, witness, seed)
         open(done, "w").write("ok\n")
     dist.barrier()
     return z, w
@@ -243,6 +262,11 @@ def config(args, n_vars, domain):
             "parallelism": f"replicas{args.gpus}"}
 
 
+def wtns_n_vars(w):
+    with open(w, "rb") as f:
+        return int.from_bytes(f.read(64)[60:64], "little")
+
+
 def cpu_baseline(z, w):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import _oracle
@@ -270,22 +294,28 @@ def traffic_per_point():
     return out
 
 
-def roofline_of(kind, rec, peak, step_ms, records_per_point=None):
-    """Algorithmic IMAD-class ops of the accumulation kernels of `kind` over
-    their measured event time, against the measured IMAD peak.  With the
-    fixed-base window count, `issued` repeats it with the ops the kernel
-    actually issues per sorted record (fewer records and cheaper products
-    than the convention counts)."""
+def roofline_of(kind, rec, peak, step_ms, records_per_point=None, peak_variants=None):
+    """IMAD-class ops of the accumulation kernels of `kind` over their
+    measured event time, against the measured carry-chain IMAD peak.  With
+    the fixed-base window count known (records_per_point), the headline
+    `achieved` / `frac` count the ops the kernel issues (records x ops per
+    record); `convention` keeps the fixed work count (reference
+    decomposition, 264 ops per product), which exceeds what the fixed-base
+    kernel issues.  `peak_variants` gives the same fraction against each
+    measured or nominal integer-pipe rate."""
     kms, kl, ku = rec
     if not kl or kms <= 0:
         return None
-    achieved = ku * FP_MULTS_PER_POINT[kind] * IMAD_PER_FP_MULT / (kms / 1e3) / 1e12
+    conv = ku * FP_MULTS_PER_POINT[kind] * IMAD_PER_FP_MULT / (kms / 1e3) / 1e12
     per_point = traffic_per_point().get(kind)
-    r = {"bound": "imad", "kernel": f"k_msm_accum0 ({kind})", "achieved": achieved,
-         "peak": peak, "unit": "TIOP/s", "frac": achieved / peak,
+    r = {"bound": "imad", "kernel": f"k_msm_accum0 ({kind})", "achieved": conv,
+         "peak": peak, "unit": "TIOP/s", "frac": conv / peak, "work": "convention",
          "traffic": per_point * ku / kl if per_point else None,
          "peak_source": "zk_imad_probe (measured carry-chain IMAD throughput)",
-         "avg_launch_ms": kms / kl, "launches": int(kl)}
+         "avg_launch_ms": kms / kl, "launches": int(kl),
+         "convention": {"achieved": conv, "frac": conv / peak,
+                        "per_point": f"{FP_MULTS_PER_POINT[kind]:.0f} Fp products x "
+                                     f"{IMAD_PER_FP_MULT:.0f} ops"}}
     if step_ms:
         r["share_of_step"] = kms / step_ms
     if records_per_point:
@@ -293,7 +323,28 @@ def roofline_of(kind, rec, peak, step_ms, records_per_point=None):
         r["issued"] = {"records_per_point": records_per_point,
                        "imad_per_record": ISSUED_IMAD_PER_RECORD[kind],
                        "achieved": ia, "frac": ia / peak}
+        r["achieved"], r["frac"], r["work"] = ia, ia / peak, "issued"
+    if peak_variants:
+        r["peak_variants"] = {k: {"peak": v, "frac": r["achieved"] / v}
+                              for k, v in peak_variants.items() if v}
     return r
+
+
+def int_peaks(L, ctx, sm_mhz):
+    """The integer-pipe rates the roofline is read against (TIOP/s): the two
+    measured probes and the nominal 64 IMAD / clock / SM at the sampled SM
+    clock."""
+    from zyklop_b200._lib import check
+    out = {}
+    for kind, name in ((0, "carry_chain_probe"), (1, "independent_mad_probe")):
+        v = ctypes.c_double()
+        check(L.zk_int_probe(ctx, kind, ctypes.byref(v)))
+        out[name] = v.value
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    if sm_mhz:
+        out["nominal_64_per_clk_per_sm"] = 64.0 * sms * sm_mhz * 1e6 / 1e12
+    return out
 
 
 def table_windows(args, tuned, group):
@@ -380,7 +431,8 @@ def run_mine(args, dist):
     # uniform scalars, not for circom-like witnesses (zero digits are skipped)
     wins = ({"accum_g1": table_windows(args, tuned, 1), "accum_g2": table_windows(args, tuned, 2)}
             if args.witness == "uniform" else {"accum_g1": None, "accum_g2": None})
-    roofline = roofline_of(dom, kinds[dom], peak.value, ms, wins[dom])
+    variants = int_peaks(L, ctx, clk.get("sm_mhz"))
+    roofline = roofline_of(dom, kinds[dom], peak.value, ms, wins[dom], variants)
     other = {k: {"ms_per_step": v[0] / args.steps, "launches": int(v[1])} for k, v in kinds.items()}
 
     # the same kernels with a proof's MSMs back to back on one stream (an
@@ -398,7 +450,7 @@ def run_mine(args, dist):
     check(L.zk_ctx_set_prove_streams(ctx, 0))
     assert np.array_equal(proof, reference_proof), "proofs changed with one MSM stream"
     skinds = {k: (prof.ms[i], prof.launches[i], prof.units[i]) for i, k in enumerate(Profile.KINDS)}
-    roofline_serial = {k: roofline_of(k, skinds[k], peak.value, None, wins[k])
+    roofline_serial = {k: roofline_of(k, skinds[k], peak.value, None, wins[k], variants)
                        for k in FP_MULTS_PER_POINT}
 
     # e2e through the one-shot host-buffer entry point
@@ -430,10 +482,10 @@ def run_mine(args, dist):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (exact Fr/Fp arithmetic)",
         "data": "synthetic (seeded circuit, CRS and witness)",
-        "config": dict(config(args, circuit.n_vars, circuit.domain),
-                       resident_crs="zkey uploaded once; fixed-base window tables built once "
-                                    f"({t_pre:.2f} s, zk_circuit_precompute)",
-                       autotuned=tuned, autotune_s=round(t_tune, 1)),
+        "config": config(args, circuit.n_vars, circuit.domain),
+        "setup": {"resident_crs": "zkey uploaded once; fixed-base window tables built once "
+                                  f"({t_pre:.2f} s, zk_circuit_precompute)",
+                  "autotuned": tuned, "autotune_s": round(t_tune, 1)},
         "e2e": {"value": args.gpus * e2e_steps / (ems / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "call": "zk_groth16_prove_files (zkey + wtns files -> proof)"},
@@ -448,7 +500,80 @@ def run_mine(args, dist):
         "gpu_launches": int(lc1.value - lc0.value),
     }
     circuit.close()
+    line["_proof"] = reference_proof.tobytes().hex()
     return line, (z, w), ctx
+
+
+def run_config2(args, dist, ctx, L):
+    """Config 2: one proof of a 2^22-constraint circuit with 1-4 nonzeros per
+    A/B row and a circom-like witness.  value: resident circuit with tuned
+    fixed-base tables and a device witness (CUDA events on the context
+    stream); e2e: the drop-in one-shot call on the files."""
+    import torch
+    from zyklop_b200 import api
+    from zyklop_b200._lib import check
+    lg = args.config2_log
+    z, w = synth_cached(args, dist, lg, "circom", 2)
+    t_tune = time.perf_counter()
+    tuned = autotune_sizes(args, api, ctx, [lg], api.SKEWED)
+    t_tune = time.perf_counter() - t_tune
+    circuit = api.Circuit(z, ctx=ctx)
+    wit = api.read_wtns(w)
+    circuit.prove(wit)  # detects the witness distribution
+    t_pre = time.perf_counter()
+    circuit.precompute(0, 0)
+    t_pre = time.perf_counter() - t_pre
+    dwit = api.to_device(wit)
+    n = wit.shape[0]
+    proof = np.zeros(32, np.uint64)
+    pp = proof.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+    stream = torch.cuda.current_stream()
+
+    def step():
+        check(L.zk_prove_device(circuit.handle, api.ptr(dwit), n, None, None, pp))
+
+    for _ in range(2):
+        step()
+    first = proof.copy()
+    clocks = ClockSampler(dist.local)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.config2_steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = dist.max(e0.elapsed_time(e1))
+    assert np.array_equal(proof, first), "config-2 proofs changed between steps"
+    circuit.close()
+    e_steps = 3
+    check(L.zk_groth16_prove_files(ctx, z.encode(), w.encode(), pp))  # warm the page cache
+    assert np.array_equal(proof, first)
+    e0.record(stream)
+    for _ in range(e_steps):
+        check(L.zk_groth16_prove_files(ctx, z.encode(), w.encode(), pp))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = dist.max(e0.elapsed_time(e1))
+    assert np.array_equal(proof, first), "one-shot config-2 proof differs from the resident one"
+    return {
+        "workload": f"groth16_prove_2^{lg}_circom",
+        "config": {"constraints": (1 << lg) - 9, "domain": 1 << lg, "n_vars": wtns_n_vars(w),
+                   "n_public": 8, "circuit": "seeded synthetic R1CS, 1-4 nnz per A/B row",
+                   "witness": "circom-like (55% in {0,1}, 15% below 2^64, 30% uniform)",
+                   "proof": "unblinded (reference-compatible)"},
+        "value": args.gpus * args.config2_steps / (ms / 1e3), "unit": UNIT,
+        "steps": args.config2_steps, "ms_per_step": ms / args.config2_steps,
+        "e2e": {"value": args.gpus * e_steps / (ems / 1e3), "unit": UNIT, "steps": e_steps,
+                "h2d_bytes_per_step": zkey_bytes(z, {4, 5, 7, 8, 9}) + os.path.getsize(w),
+                "d2h_bytes_per_step": 3 * 2 * 128 * 17 + 2 * 256 * 17,
+                "call": "zk_groth16_prove_files (zkey + wtns files -> proof)"},
+        "setup": {"autotuned": tuned, "autotune_s": round(t_tune, 1),
+                  "tables_s": round(t_pre, 2)},
+        "clocks": clk,
+        "_proof": first.tobytes().hex(),
+    }
 
 
 # -------------------------------------------------------------- primitives
@@ -459,23 +584,40 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def prim_inputs(group, log_max, seed):
-    """Points k_i * G (device, SoA) and uniform scalars for the sweep."""
-    from zyklop_b200 import api
-    rng = np.random.default_rng(seed)
-    n = 1 << log_max
-    k = rng.integers(0, 2**63, size=(n, 4), dtype=np.uint64)
-    k[:, 3] &= np.uint64((1 << 60) - 1)
-    px, py = api.mul_generator(group, k, keep_on_device=True)
-    s = rng.integers(0, 2**63, size=(n, 4), dtype=np.uint64)
-    s[:, 3] &= np.uint64((1 << 60) - 1)
-    return px, py, api.to_device(s)
-
-
-def time_calls(fn, reps=3):
+def prim_inputs(args, group, log_max, seed):
+    """Points k_i * G (device, SoA; written by zk_synth in a child process)
+    and uniform scalars below 2^252 (numpy, seeded) for the sweep."""
     import torch
+    d = os.path.join(args.workdir, "prims")
+    os.makedirs(d, exist_ok=True)
+    fx = os.path.join(d, f"g{group}_l{log_max}_s{seed}_x.bin")
+    fy = os.path.join(d, f"g{group}_l{log_max}_s{seed}_y.bin")
+    if not (os.path.exists(fx) and os.path.exists(fy)):
+        run_synth("points", group, log_max, seed, fx, fy)
+    px = torch.from_numpy(np.fromfile(fx, dtype=np.int64)).cuda()
+    py = torch.from_numpy(np.fromfile(fy, dtype=np.int64)).cuda()
+    return px, py, torch.from_numpy(seeded_fr(1 << log_max, seed).view(np.int64)).cuda()
+
+
+def seeded_fr(n, seed, top_bits=60):
+    """n x 4 u64 values below 2^(192 + top_bits) from a seeded numpy stream."""
+    rng = np.random.default_rng(seed)
+    s = rng.integers(0, 2**63, size=(n, 4), dtype=np.uint64) * np.uint64(2) + \
+        rng.integers(0, 2, size=(n, 4), dtype=np.uint64)
+    s[:, 3] &= np.uint64((1 << top_bits) - 1)
+    return s
+
+
+PRIM_REPS = 3  # timed calls per primitive size (0: one untimed call, for parity only)
+
+
+def time_calls(fn, reps=None):
+    import torch
+    reps = PRIM_REPS if reps is None else min(reps, PRIM_REPS)
     fn()
     torch.cuda.synchronize()
+    if reps == 0:
+        return float("nan")
     ts = []
     for _ in range(reps):
         t = time.perf_counter()
@@ -485,44 +627,86 @@ def time_calls(fn, reps=3):
     return float(np.median(ts))
 
 
-def run_primitives(args, msm_fns, ntt_fn, imad_peak):
+def digest(t):
+    """sha256 of a device buffer's bytes (compares large outputs across arms)."""
+    import hashlib
+    return hashlib.sha256(t.cpu().numpy().tobytes()).hexdigest()[:32]
+
+
+def run_primitives(args, msm_fns, ntt_fn, hpoly_fn, imad_peak):
     """Config-1 sweep: G1 MSM at 2^18..2^24 and G2 MSM at 2^18, 2^20 (uniform
-    scalars, points k_i G), Fr NTT at 2^16..2^24.  msm_fns[g](px, py, sc, n)
-    and ntt_fn(buf, log_n) are the implementation's calls on device buffers."""
+    scalars, points k_i G), Fr NTT and INTT at 2^16..2^24, and the H pipeline
+    (three coset INTT / NTT pairs) at a few sizes.  msm_fns[g](px, py, sc, n)
+    returns the result as hex; ntt_fn(buf, log_n, inverse) and
+    hpoly_fn(a, b, c, log_n, h) run in place on device buffers.  Returns the
+    timings and, under "outputs", every result (MSM points as hex, NTT / H
+    outputs as sha256 digests) for the parity check between arms."""
     import torch
-    out = {"g1_msm": {}, "g2_msm": {}, "ntt": {}}
+    out = {"g1_msm": {}, "g2_msm": {}, "ntt": {}, "intt": {}, "hpoly": {}}
+    outputs = {"g1_msm": {}, "g2_msm": {}, "ntt": {}, "intt": {}, "hpoly": {}}
     peak_hbm, hbm_src = hbm_peak()
     for g, logs in ((1, [int(x) for x in args.prim_g1.split(",") if x]),
                     (2, [int(x) for x in args.prim_g2.split(",") if x])):
         if not logs:
             continue
-        px, py, sc = prim_inputs(g, max(logs), 40 + g)
+        px, py, sc = prim_inputs(args, g, max(logs), 40 + g)
         for lg in logs:
             n = 1 << lg
-            t = time_calls(lambda: msm_fns[g](px, py, sc, n))
+            res = {}
+            t = time_calls(lambda: res.__setitem__("r", msm_fns[g](px, py, sc, n)))
             per_point = FP_MULTS_PER_POINT["accum_g1" if g == 1 else "accum_g2"]
             r = {"ms": t * 1e3, "points_per_s": n / t}
             if imad_peak:
                 r["imad_frac"] = n * per_point * IMAD_PER_FP_MULT / t / 1e12 / imad_peak
             out[f"g{g}_msm"][f"2^{lg}"] = r
+            outputs[f"g{g}_msm"][f"2^{lg}"] = res["r"]
         del px, py, sc
         torch.cuda.empty_cache()
     for lg in [int(x) for x in args.prim_ntt.split(",") if x]:
         n = 1 << lg
-        buf = torch.randint(0, 2**62, (n, 4), dtype=torch.int64, device="cuda")
-        buf[:, 3] &= (1 << 58) - 1  # canonical Fr, read as Montgomery
-        t = time_calls(lambda: ntt_fn(buf, lg))
-        r = {"ms": t * 1e3, "gb_per_s": 64 * n / t / 1e9, "hbm_frac": 64 * n / t / 1e9 / peak_hbm}
-        if imad_peak:  # one twiddle product per butterfly: (n / 2) log2 n products
-            r["imad_frac"] = (n // 2) * lg * IMAD_PER_FP_MULT / t / 1e12 / imad_peak
-        out["ntt"][f"2^{lg}"] = r
-        del buf
+        src = torch.from_numpy(seeded_fr(n, 500 + lg, 58).view(np.int64)).cuda()
+        for inverse, key in ((False, "ntt"), (True, "intt")):
+            buf = src.clone()
+            t = time_calls(lambda: ntt_fn(buf, lg, inverse), reps=3)
+            # parity: one transform of the seeded input
+            buf.copy_(src)
+            ntt_fn(buf, lg, inverse)
+            torch.cuda.synchronize()
+            outputs[key][f"2^{lg}"] = digest(buf)
+            r = {"ms": t * 1e3, "gb_per_s": 64 * n / t / 1e9, "hbm_frac": 64 * n / t / 1e9 / peak_hbm}
+            if imad_peak:  # one twiddle product per butterfly: (n / 2) log2 n products
+                r["imad_frac"] = (n // 2) * lg * IMAD_PER_FP_MULT / t / 1e12 / imad_peak
+            out[key][f"2^{lg}"] = r
+            del buf
+        del src
+    for lg in [int(x) for x in args.prim_hpoly.split(",") if x]:
+        if hpoly_fn is None:
+            break
+        n = 1 << lg
+        a0 = torch.from_numpy(seeded_fr(n, 700 + lg, 58).view(np.int64)).cuda()
+        b0 = torch.from_numpy(seeded_fr(n, 800 + lg, 58).view(np.int64)).cuda()
+        a, b = a0.clone(), b0.clone()
+        c, h = torch.empty_like(a0), torch.empty_like(a0)
+
+        def once():
+            a.copy_(a0)
+            b.copy_(b0)
+            hpoly_fn(a, b, c, lg, h)
+        t = time_calls(once)
+        outputs["hpoly"][f"2^{lg}"] = digest(h)
+        # 3 INTT + 3 NTT (64 B per element each) + pointwise / coset / h passes
+        out["hpoly"][f"2^{lg}"] = {"ms": t * 1e3, "elements_per_s": n / t,
+                                   "transforms": "3 coset INTT/NTT pairs + glue"}
+        del a0, b0, a, b, c, h
+        torch.cuda.empty_cache()
     out["conventions"] = (f"MSM work {FP_MULTS_PER_POINT['accum_g1']:.0f} (G1) / "
                           f"{FP_MULTS_PER_POINT['accum_g2']:.0f} (G2) Fp products per point x "
                           f"{IMAD_PER_FP_MULT:.0f} IMAD-class ops against the measured IMAD "
                           f"probe; NTT bytes 64 per element against HBM {peak_hbm:.0f} GB/s "
                           f"({hbm_src}) and (n/2) log2 n products against the IMAD probe; "
-                          "wall time of the API call, inputs resident")
+                          "wall time of the API call, inputs resident (the H pipeline call "
+                          "includes copying its two inputs back in)")
+    out["outputs"] = outputs
     return out
 
 
@@ -532,16 +716,23 @@ def mine_primitives(args, ctx, L, imad_peak):
     res = np.zeros(16, np.uint64)
     inf = ctypes.c_int()
 
-    def msm(fn):
-        return lambda px, py, sc, n: check(fn(ctx, api.ptr(px), api.ptr(py), api.ptr(sc), n,
-                                              res.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
-                                              ctypes.byref(inf)))
+    def msm(fn, width):
+        def call(px, py, sc, n):
+            check(fn(ctx, api.ptr(px), api.ptr(py), api.ptr(sc), n,
+                     res.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), ctypes.byref(inf)))
+            return res[:width].tobytes().hex()
+        return call
 
-    def ntt(buf, lg):
-        check(L.zk_ntt(ctx, api.ptr(buf), lg, 0))
+    def ntt(buf, lg, inverse):
+        check(L.zk_ntt(ctx, api.ptr(buf), lg, 1 if inverse else 0))
 
-    out = run_primitives(args, {1: msm(L.zk_msm_g1), 2: msm(L.zk_msm_g2)}, ntt, imad_peak)
-    out["calls"] = "zk_msm_g1 / zk_msm_g2 (windowed, autotuned where tuned), zk_ntt (forward)"
+    def hpoly(a, b, c, lg, h):
+        check(L.zk_hpoly(ctx, api.ptr(a), api.ptr(b), lg, api.ptr(h)))
+
+    out = run_primitives(args, {1: msm(L.zk_msm_g1, 8), 2: msm(L.zk_msm_g2, 16)}, ntt, hpoly,
+                         imad_peak)
+    out["calls"] = ("zk_msm_g1 / zk_msm_g2 (windowed, autotuned where tuned), zk_ntt (forward and "
+                    "inverse), zk_hpoly")
     return out
 
 
@@ -786,64 +977,166 @@ def run_serving(args, dist, ctx, L):
 
 
 # ------------------------------------------------------------- reference
-def run_reference(args, dist):
-    import torch
-    torch.cuda.set_device(dist.local)
+def reference_prove_lib():
     lib_path = os.path.join(ROOT, "oracle", "_ref", "libzkref_prove.so")
     if not os.path.exists(lib_path):
-        return {"impl": "reference", "unavailable":
-                "reference sm_100a build missing (oracle/_ref; make -C oracle/refbuild)"}
-    z, w = circuit_files(args, dist)
+        return None
     L = ctypes.CDLL(lib_path)
     L.zkref_prove_files.argtypes = [ctypes.c_char_p, ctypes.c_char_p,
                                     ctypes.POINTER(ctypes.c_uint64)]
+    return L
+
+
+def reference_proofs(L, z, w, steps, warmup, stream):
+    """groth16Prove of the reference build on (z, w): `warmup` untimed and
+    `steps` timed proofs (CUDA events on the current stream around host
+    calls that synchronize).  Returns (ms, proof)."""
+    import torch
     proof = np.zeros(32, np.uint64)
     pp = proof.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
-
-    def step():
-        L.zkref_prove_files(z.encode(), w.encode(), pp)
-
     with silenced():
-        for _ in range(args.warmup):
-            step()
+        for _ in range(max(warmup, 1 if steps == 0 else 0)):
+            L.zkref_prove_files(z.encode(), w.encode(), pp)
     torch.cuda.synchronize()
-    clocks = ClockSampler(dist.local)
-    dist.barrier()
-    stream = torch.cuda.current_stream()
+    if steps == 0:
+        return None, proof
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with silenced():
         start.record(stream)
-        for _ in range(args.steps):
-            step()
+        for _ in range(steps):
+            L.zkref_prove_files(z.encode(), w.encode(), pp)
         end.record(stream)
         torch.cuda.synchronize()
+    return start.elapsed_time(end), proof
+
+
+def ref_outputs_path(args):
+    return os.path.join(args.workdir, "ref_outputs.json")
+
+
+def run_reference(args, dist):
+    """The reference arm: its groth16Prove on the config-0 circuit (timed
+    steps), on the config-2 circuit (a few timed steps), and its primitive
+    sweep; every result goes to ref_outputs.json in the work directory."""
+    import torch
+    torch.cuda.set_device(dist.local)
+    L = reference_prove_lib()
+    if L is None:
+        return {"impl": "reference", "unavailable":
+                "reference sm_100a build missing (oracle/_ref; make -C oracle/refbuild)"}
+    z, w = circuit_files(args, dist)
+    stream = torch.cuda.current_stream()
+    record = {"workdir_inputs": {"config0": [z, w]}}
+    if args.parity_only:
+        _, proof = reference_proofs(L, z, w, 0, 1, stream)
+        record["proof_2^%d" % args.log_domain] = proof.tobytes().hex()
+        if args.config2_log:
+            z2, w2 = synth_cached(args, dist, args.config2_log, "circom", 2)
+            _, p2 = reference_proofs(L, z2, w2, 0, 1, stream)
+            record["proof_2^%d" % args.config2_log] = p2.tobytes().hex()
+        global PRIM_REPS
+        PRIM_REPS = 0
+        prims = reference_primitives(args)
+        record["primitives"] = prims["outputs"] if prims else {}
+        json.dump(record, open(ref_outputs_path(args), "w"))
+        return None
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    ms, proof = reference_proofs(L, z, w, args.steps, args.warmup, stream)
     dist.barrier()
     clk = clocks.stop()
-    ms = dist.max(start.elapsed_time(end))
+    ms = dist.max(ms)
     value = args.gpus * args.steps / (ms / 1e3)
-    n_vars = int.from_bytes(open(w, "rb").read()[60:64], "little")
+    record["proof_2^%d" % args.log_domain] = proof.tobytes().hex()
+    record["value"] = value
+    config2 = None
+    if args.config2_log:
+        z2, w2 = synth_cached(args, dist, args.config2_log, "circom", 2)
+        k2 = max(1, min(args.steps, 3))
+        ms2, p2 = reference_proofs(L, z2, w2, k2, 1, stream)
+        record["proof_2^%d" % args.config2_log] = p2.tobytes().hex()
+        config2 = {"workload": f"groth16_prove_2^{args.config2_log}_circom",
+                   "value": k2 / (ms2 / 1e3), "unit": UNIT, "steps": k2,
+                   "ms_per_step": ms2 / k2,
+                   "call": "groth16Prove (zkey + wtns files -> proof), every step a full proof"}
+        record["config2_value"] = config2["value"]
     prims = reference_primitives(args)
-    return {
+    if prims:
+        record["primitives"] = prims["outputs"]
+    json.dump(record, open(ref_outputs_path(args), "w"))
+    line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64 limbs (exact Fr/Fp arithmetic)",
         "data": "synthetic (seeded circuit, CRS and witness)",
-        "config": config(args, n_vars, 1 << args.log_domain),
+        "config": config(args, wtns_n_vars(w), 1 << args.log_domain),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 8, "kind": "reference",
                          "sample": "the reference's own sm_100a build (groth16Prove from "
                                    "zkey/wtns files; GPU kernels + 8 OpenMP host threads), "
                                    "every step a full proof"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "clocks": clk,
+        "config2": config2,
         "primitives": prims,
+        "inputs": "written by zyklop_b200/bin/zk_synth in a child process; this process loads "
+                  "only the reference build (oracle/_ref)",
     }
+    return line
+
+
+def reference_outputs(args):
+    """The reference build's results on this run's inputs: ref_outputs.json
+    as the reference arm left it in the work directory, else made now by the
+    reference build in a child process (bench.py --impl reference
+    --parity-only).  Returns (outputs, source)."""
+    path = ref_outputs_path(args)
+    want = ["proof_2^%d" % args.log_domain] + (
+        ["proof_2^%d" % args.config2_log] if args.config2_log else [])
+    if os.path.exists(path):
+        rec = json.load(open(path))
+        if all(k in rec for k in want):
+            return rec, "the reference arm's outputs (ref_outputs.json, same inputs)"
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--parity-only",
+           "--workdir", args.workdir, "--log-domain", str(args.log_domain),
+           "--config2-log", str(args.config2_log), "--prim-g1", args.prim_g1,
+           "--prim-g2", args.prim_g2, "--prim-ntt", args.prim_ntt,
+           "--prim-hpoly", args.prim_hpoly]
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1200)
+    if r.returncode != 0 or not os.path.exists(path):
+        return None, "reference build failed: " + r.stderr.strip()[-300:]
+    return json.load(open(path)), "the reference build run in a child process (--parity-only)"
+
+
+def parity_report(mine, ref, source):
+    """Bit-equality of this arm's results with the reference build's, per
+    item; None where the reference has no result for it."""
+    if ref is None:
+        return {"checked": False, "source": source}
+    out = {"source": source}
+    ok = True
+    for k, v in mine.items():
+        if isinstance(v, dict):
+            sub = {}
+            for kk, vv in v.items():
+                theirs = ref.get("primitives", {}).get(k, {}).get(kk)
+                sub[kk] = None if theirs is None else theirs == vv
+                ok = ok and sub[kk] is not False
+            out[k] = sub
+        else:
+            theirs = ref.get(k)
+            out[k] = None if theirs is None else theirs == v
+            ok = ok and out[k] is not False
+    out["all_equal"] = ok
+    return out
 
 
 def reference_primitives(args):
     """The same config-1 sweep through the reference build's own primitives
-    (msm_g1, msm_g2_device, ntt) on device buffers."""
+    (msm_g1, msm_g2_device, ntt, computeHPoly) on device buffers."""
     path = os.path.join(ROOT, "oracle", "_ref", "libzkref_prims.so")
+    ipath = os.path.join(ROOT, "oracle", "_ref", "libzkref_inter.so")
     if not os.path.exists(path) or not (args.prim_g1 or args.prim_g2 or args.prim_ntt):
         return None
     u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -854,22 +1147,36 @@ def reference_primitives(args):
         fn.restype = ctypes.c_int
     L.zkref_ntt_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     L.zkref_ntt_device.restype = ctypes.c_int
+    hp = None
+    if os.path.exists(ipath):
+        IL = ctypes.CDLL(ipath)
+        if hasattr(IL, "zkref_hpoly_device"):
+            hp = IL.zkref_hpoly_device
+            hp.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_void_p]
+            hp.restype = ctypes.c_int
     out = np.zeros(16, np.uint64)
 
-    def msm(fn):
+    def msm(fn, width):
         def call(px, py, sc, n):
             with silenced():
                 fn(ctypes.c_void_p(px.data_ptr()), ctypes.c_void_p(py.data_ptr()),
                    ctypes.c_void_p(sc.data_ptr()), n, out.ctypes.data_as(u64p))
+            return out[:width].tobytes().hex()
         return call
 
-    def ntt(buf, lg):
+    def ntt(buf, lg, inverse):
         with silenced():
-            L.zkref_ntt_device(ctypes.c_void_p(buf.data_ptr()), lg, 0)
+            L.zkref_ntt_device(ctypes.c_void_p(buf.data_ptr()), lg, 1 if inverse else 0)
 
-    r = run_primitives(args, {1: msm(L.zkref_msm_g1_device), 2: msm(L.zkref_msm_g2_device)},
-                       ntt, None)
-    r["calls"] = "the reference's msm_g1, msm_g2_device and ntt (oracle/_ref/libzkref_prims.so)"
+    def hpoly(a, b, c, lg, h):
+        with silenced():
+            hp(*[ctypes.c_void_p(t.data_ptr()) for t in (a, b, c)], lg, ctypes.c_void_p(h.data_ptr()))
+
+    r = run_primitives(args, {1: msm(L.zkref_msm_g1_device, 8), 2: msm(L.zkref_msm_g2_device, 16)},
+                       ntt, hpoly if hp else None, None)
+    r["calls"] = ("the reference's msm_g1, msm_g2_device, ntt (oracle/_ref/libzkref_prims.so) and "
+                  "computeHPoly (oracle/_ref/libzkref_inter.so); each call includes the "
+                  "reference's own nttPrepare / nttDestroy")
     return r
 
 
@@ -888,11 +1195,17 @@ def main():
         os.environ["WORLD_SIZE"] = "1"
         dist = Dist()
         line = run_reference(args, dist)
-        print(json.dumps(line), flush=True)
+        if line is not None:
+            print(json.dumps(line), flush=True)
         return
     dist = Dist()
     try:
         line, files, ctx = run_mine(args, dist)
+        mine_out = {"proof_2^%d" % args.log_domain: line.pop("_proof")}
+        if dist.world == 1 and args.config2_log:
+            c2 = run_config2(args, dist, ctx, lib_handle())
+            mine_out["proof_2^%d" % args.config2_log] = c2.pop("_proof")
+            line["config2"] = c2
         if dist.world == 1 and args.batch_proofs > 0:
             line["batched"] = run_batched(args, dist, ctx, lib_handle())
         if dist.world == 1 and args.serve_seconds > 0:
@@ -900,6 +1213,7 @@ def main():
         if dist.world == 1 and (args.prim_g1 or args.prim_g2 or args.prim_ntt):
             line["primitives"] = mine_primitives(args, ctx, lib_handle(),
                                                  line["roofline"]["peak"])
+            mine_out.update(line["primitives"].pop("outputs"))
             if not args.no_cpu_baseline:
                 cb = cpu_msm_baseline()
                 if cb:
@@ -907,6 +1221,11 @@ def main():
         lib_handle().zk_ctx_destroy(ctx)
         if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(*files)
+        if dist.rank == 0 and dist.world == 1:
+            ref, source = reference_outputs(args)
+            line["parity_vs_reference"] = parity_report(mine_out, ref, source)
+            if ref and "config2" in line and "config2_value" in ref:
+                line["config2"]["reference_value"] = ref["config2_value"]
         if dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

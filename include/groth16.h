@@ -30,6 +30,17 @@ struct Groth16ZkeyHeader {
   uint64_t prime[4];
 };
 
+/* include/groth16.cuh:93-98: one section-4 coefficient as a caller holds it
+ * in memory (matrix 0 = A, 1 = B, 2 = C).  Declared for source compatibility;
+ * the prover reads section 4 straight from the zkey and takes no array of
+ * these (groth16SparseMvm, the reference's only user, is not provided). */
+struct Groth16CoefEntry {
+  uint8_t matrix;
+  uint32_t constraint;
+  uint32_t signal;
+  uint64_t value[4];
+};
+
 /* include/groth16.cuh:119-123 */
 void groth16Prove(const char* zkey_path, const char* wtns_path, Groth16Proof& proof);
 /* include/groth16.cuh:149-153 */

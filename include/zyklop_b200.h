@@ -62,6 +62,19 @@ int zk_ctx_set_stream(zk_ctx* ctx, void* stream);
  * device to the driver. */
 int zk_release_cached_memory(zk_ctx* ctx);
 
+/* Allocations the library has made in this process so far (device blocks
+ * and their bytes, pinned host buffers), and the reserved / in-use bytes of
+ * its memory pool on `device` (0 when that device has none yet).  For
+ * checking that a call allocates nothing.  No reference counterpart. */
+typedef struct {
+  uint64_t device_allocations;
+  uint64_t device_allocated_bytes;
+  uint64_t pinned_allocations;
+  uint64_t pool_reserved_bytes;
+  uint64_t pool_used_bytes;
+} zk_memory_stats_t;
+int zk_memory_stats(int device, zk_memory_stats_t* out);
+
 /* ---- measurement ----------------------------------------------------------- */
 /* Number of kernels this library has launched in the process so far. */
 int zk_launch_count(uint64_t* out);
@@ -85,6 +98,11 @@ int zk_ctx_profile(zk_ctx* ctx, zk_profile* out);
  * the field multiplication's instruction mix), in 10^12 ops/s: the
  * denominator of the MSM roofline.  No reference counterpart. */
 int zk_imad_probe(zk_ctx* ctx, double* tiops);
+/* The same measurement for kind 0 (carry chains, = zk_imad_probe) or kind 1
+ * (independent mad.lo / mad.hi streams without carries: the integer pipe's
+ * rate when no carry flag serializes the instructions).  No reference
+ * counterpart. */
+int zk_int_probe(zk_ctx* ctx, int kind, double* tiops);
 
 /* ---- field primitives (device pointers, n elements of 4 x u64) ----------- */
 #define ZK_FIELD_FP 0
@@ -139,10 +157,15 @@ int zk_msm_g2(zk_ctx* ctx, const uint64_t* d_px, const uint64_t* d_py, const uin
  * zk_msm_g1, on the caller's `stream` (a cudaStream_t; NULL = default
  * stream); blocks until the result is on the host.  Its scratch is a fixed
  * 24 MiB __device__ array, so n is limited to 65536 points (larger n returns
- * ZK_EINVAL).  The first call on each device looks up that array's address
- * once; make it before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race, so serialize them.  No counterpart in the
- * reference. */
+ * ZK_EINVAL).  CUDA loads a library's device code lazily, so that array
+ * takes device memory when a device first runs this call (which also looks
+ * up the array's address), not when the library loads: make one warm-up
+ * call on each device before the host application's pool claims the
+ * device's memory (if the array cannot be placed, the call fails with
+ * ZK_ENOMEM and says so).  The call synchronizes its stream, so it cannot
+ * run while that stream is being captured into a CUDA graph (ZK_ENOTSUP).
+ * All calls share the array: calls that overlap on the GPU race, so
+ * serialize them.  No counterpart in the reference. */
 int zk_msm_g1_noalloc(const uint64_t* d_px, const uint64_t* d_py, const uint64_t* d_scalars,
                       size_t n, uint64_t* h_out, int* is_inf, void* stream);
 
@@ -311,6 +334,38 @@ int zk_server_destroy(zk_server* srv);
  * For checking the pipeline's intermediates. */
 int zk_prove_intermediates(zk_circuit* c, const uint64_t* h_witness, size_t n_witness,
                            uint64_t* aw, uint64_t* bw, uint64_t* h, uint64_t* proof);
+
+/* Every intermediate of an unblinded proof, for comparing the pipeline step
+ * by step with the reference prover's own (src/groth16.cu:1143-1397).  The
+ * caller sets the buffer pointers it wants (host memory, domain x 4 u64
+ * each; NULL skips) and the call fills them and the MSM results:
+ *   aw, bw       A.w, B.w (Montgomery), readAndComputeMVM's outputs
+ *                (src/groth16.cu:737-861);
+ *   ea, eb, ec   A, B and C = A.B evaluated on the odd coset
+ *                omega_2n^(2j+1) (Montgomery, natural order), the buffers
+ *                computeHPoly leaves after its forward NTTs
+ *                (src/groth16.cu:1037-1128);
+ *   h            h_j = (A.B - C)(omega_2n^(2j+1)), canonical;
+ *   msm_*        the four MSM results, affine Montgomery: A (alpha1
+ *                included), B2 (beta2 included), the C part and the H part
+ *                of pi_C (src/groth16.cu:1329-1389); inf[k] = 1 where a
+ *                result is the point at infinity.
+ * The proof is the same as zk_prove's. */
+typedef struct {
+  uint64_t* aw;
+  uint64_t* bw;
+  uint64_t* ea;
+  uint64_t* eb;
+  uint64_t* ec;
+  uint64_t* h;
+  uint64_t msm_a[8];
+  uint64_t msm_b2[16];
+  uint64_t msm_c[8];
+  uint64_t msm_h[8];
+  int32_t inf[4];
+} zk_prove_trace;
+int zk_prove_traced(zk_circuit* c, const uint64_t* h_witness, size_t n_witness,
+                    zk_prove_trace* trace, uint64_t* proof);
 
 /* One-shot proof from zkey + wtns files / in-memory images (the circuit is
  * loaded, used and released inside the call).  Replaces

@@ -29,4 +29,15 @@ int zkref_proof_json(const uint64_t* in, char* out, size_t out_size) {
   return 0;
 }
 
+// 256-byte EVM calldata of a proof given in the reference layout
+// (groth16ProofToCalldata, src/groth16.cu:1514-1557).
+int zkref_proof_calldata(const uint64_t* in, uint8_t* out, size_t out_size) {
+  Groth16Proof p;
+  memcpy(p.pi_A, in, 64);
+  memcpy(p.pi_B, in + 8, 128);
+  memcpy(p.pi_C, in + 24, 64);
+  groth16ProofToCalldata(p, out, out_size);
+  return 0;
+}
+
 }  // extern "C"

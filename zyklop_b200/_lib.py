@@ -29,9 +29,11 @@ SIGNATURES = {
     "zk_ctx_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "zk_release_cached_memory": (ctypes.c_int, [ctypes.c_void_p]),
     "zk_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64)]),
+    "zk_memory_stats": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p]),
     "zk_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "zk_ctx_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "zk_imad_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "zk_int_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "zk_field_op": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p, sz]),
     "zk_ntt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int]),
@@ -70,6 +72,8 @@ SIGNATURES = {
     "zk_prove_intermediates": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               u64p]),
+    "zk_prove_traced": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, sz, ctypes.c_void_p,
+                                       u64p]),
     "zk_prove_batch": (ctypes.c_int, [ctypes.c_void_p, sz, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                       ctypes.c_void_p, u64p, ctypes.c_int]),
@@ -113,6 +117,32 @@ class ZkeyHeader(ctypes.Structure):
     _fields_ = [("n_constraints", ctypes.c_uint32), ("n_vars", ctypes.c_uint32),
                 ("n_public", ctypes.c_uint32), ("domain_size", ctypes.c_uint32),
                 ("log_domain", ctypes.c_int32), ("prime", ctypes.c_uint64 * 4)]
+
+
+class MemoryStats(ctypes.Structure):
+    """zk_memory_stats_t"""
+    _fields_ = [("device_allocations", ctypes.c_uint64),
+                ("device_allocated_bytes", ctypes.c_uint64),
+                ("pinned_allocations", ctypes.c_uint64),
+                ("pool_reserved_bytes", ctypes.c_uint64), ("pool_used_bytes", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+def memory_stats(device=0):
+    s = MemoryStats()
+    check(lib().zk_memory_stats(device, ctypes.byref(s)))
+    return s.as_dict()
+
+
+class ProveTrace(ctypes.Structure):
+    """zk_prove_trace: buffer pointers in, MSM results out."""
+    _fields_ = [("aw", ctypes.c_void_p), ("bw", ctypes.c_void_p), ("ea", ctypes.c_void_p),
+                ("eb", ctypes.c_void_p), ("ec", ctypes.c_void_p), ("h", ctypes.c_void_p),
+                ("msm_a", ctypes.c_uint64 * 8), ("msm_b2", ctypes.c_uint64 * 16),
+                ("msm_c", ctypes.c_uint64 * 8), ("msm_h", ctypes.c_uint64 * 8),
+                ("inf", ctypes.c_int32 * 4)]
 
 
 class TuneResult(ctypes.Structure):

@@ -184,6 +184,27 @@ class Circuit:
                                            proof.ctypes.data_as(_u64p)))
         return aw, bw, h, proof
 
+    def trace(self, witness):
+        """Every intermediate of the unblinded proof (zk_prove_traced): a dict
+        of A.w, B.w, the odd-coset evaluations of A, B, C, h (domain x 4
+        arrays), the four MSM results (msm_a, msm_b2, msm_c, msm_h), their
+        infinity flags and the proof."""
+        from ._lib import ProveTrace
+        w = np.ascontiguousarray(witness, dtype=np.uint64).reshape(-1, 4)
+        bufs = {k: np.zeros((self.domain, 4), np.uint64) for k in ("aw", "bw", "ea", "eb", "ec", "h")}
+        t = ProveTrace()
+        for k, b in bufs.items():
+            setattr(t, k, b.ctypes.data)
+        proof = np.zeros(32, dtype=np.uint64)
+        check(lib().zk_prove_traced(self.handle, w.ctypes.data_as(ctypes.c_void_p), w.shape[0],
+                                    ctypes.byref(t), proof.ctypes.data_as(_u64p)))
+        out = dict(bufs)
+        for k, n in (("msm_a", 8), ("msm_b2", 16), ("msm_c", 8), ("msm_h", 8)):
+            out[k] = np.array(list(getattr(t, k)), dtype=np.uint64)
+        out["inf"] = [int(x) for x in t.inf]
+        out["proof"] = proof
+        return out
+
     def close(self):
         if self.handle:
             lib().zk_circuit_free(self.handle)

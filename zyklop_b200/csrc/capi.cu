@@ -119,6 +119,14 @@ int zk_release_cached_memory(zk_ctx* ctx) {
   ZK_API_END
 }
 
+int zk_memory_stats(int device, zk_memory_stats_t* out) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(out, ZK_EINVAL, "zk_memory_stats: NULL output");
+  alloc_stats(&out->device_allocations, &out->device_allocated_bytes, &out->pinned_allocations);
+  pool_usage(device, &out->pool_reserved_bytes, &out->pool_used_bytes);
+  ZK_API_END
+}
+
 int zk_launch_count(uint64_t* out) {
   ZK_API_BEGIN
   ZK_REQUIRE(out, ZK_EINVAL, "zk_launch_count: NULL output");
@@ -150,6 +158,15 @@ int zk_imad_probe(zk_ctx* ctx, double* tiops) {
   ctx = resolve_ctx(ctx);
   std::lock_guard<std::mutex> g(ctx->mu);
   *tiops = imad_probe(ctx->stream);
+  ZK_API_END
+}
+
+int zk_int_probe(zk_ctx* ctx, int kind, double* tiops) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(tiops && (kind == 0 || kind == 1), ZK_EINVAL, "zk_int_probe: kind must be 0 or 1");
+  ctx = resolve_ctx(ctx);
+  std::lock_guard<std::mutex> g(ctx->mu);
+  *tiops = imad_probe(ctx->stream, kind);
   ZK_API_END
 }
 

@@ -167,6 +167,28 @@ int zk_prove_intermediates(zk_circuit* c, const uint64_t* h_witness, size_t n_wi
   ZK_API_END
 }
 
+int zk_prove_traced(zk_circuit* c, const uint64_t* h_witness, size_t n_witness,
+                    zk_prove_trace* trace, uint64_t* proof) {
+  ZK_API_BEGIN
+  ZK_REQUIRE(c && trace && proof, ZK_EINVAL, "zk_prove_traced: NULL argument");
+  enter_ctx(c->ctx);
+  std::lock_guard<std::mutex> g(c->ctx->mu);
+  ProveIntermediates dbg;
+  dbg.aw = trace->aw;
+  dbg.bw = trace->bw;
+  dbg.ea = trace->ea;
+  dbg.eb = trace->eb;
+  dbg.ec = trace->ec;
+  dbg.h = trace->h;
+  prove(c, h_witness, n_witness, false, nullptr, nullptr, proof, &dbg);
+  memcpy(trace->msm_a, dbg.msm_a, sizeof dbg.msm_a);
+  memcpy(trace->msm_b2, dbg.msm_b2, sizeof dbg.msm_b2);
+  memcpy(trace->msm_c, dbg.msm_c, sizeof dbg.msm_c);
+  memcpy(trace->msm_h, dbg.msm_h, sizeof dbg.msm_h);
+  for (int k = 0; k < 4; k++) trace->inf[k] = dbg.inf[k];
+  ZK_API_END
+}
+
 int zk_prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* circuits,
                    const uint64_t* const* witnesses, const size_t* n_witness, int on_device,
                    const uint64_t* r, const uint64_t* s, uint64_t* proofs, int inflight) {

@@ -10,10 +10,11 @@ namespace {
 std::atomic<uint64_t> g_launches{0};
 thread_local Profiler* g_prof = nullptr;
 
-// Each thread runs `iters` blocks of 16 independent mad.lo.cc / madc.hi.cc
-// carry chains over 8 register pairs: the instruction mix of the Montgomery
-// rows in field.cuh.  Results are folded into one store so nothing is
-// eliminated.
+// Each thread runs kProbeIters blocks of two 8-instruction mad.lo.cc /
+// madc.hi.cc carry chains over 8 accumulators: the instruction mix of the
+// Montgomery rows in field.cuh, where every instruction of a row waits for
+// the carry of the one before.  Results are folded into one store so
+// nothing is eliminated.
 constexpr int kProbeIters = 2048;
 
 __global__ void __launch_bounds__(256) k_imad_probe(uint32_t seed, uint32_t* out) {
@@ -44,6 +45,40 @@ __global__ void __launch_bounds__(256) k_imad_probe(uint32_t seed, uint32_t* out
   }
   const uint32_t x = t0 ^ t1 ^ t2 ^ t3 ^ t4 ^ t5 ^ t6 ^ t7;
   if (x == 0x12345678u) out[0] = x;  // practically never taken; keeps the work live
+}
+
+// The same count of multiply-adds without carries: 16 mad.lo / mad.hi per
+// iteration over 8 accumulators, so each thread keeps 8 independent
+// dependency chains in flight (the integer pipe's own rate, with no carry
+// flag serializing the chain).
+__global__ void __launch_bounds__(256) k_imad_probe_free(uint32_t seed, uint32_t* out) {
+  uint32_t a0 = seed ^ threadIdx.x, a1 = a0 * 3u + 1u, a2 = a1 * 5u + 7u, a3 = a2 * 9u + 3u;
+  uint32_t t0 = a0 + 11u, t1 = a1 + 13u, t2 = a2 + 17u, t3 = a3 + 19u;
+  uint32_t t4 = t0 ^ 5u, t5 = t1 ^ 7u, t6 = t2 ^ 9u, t7 = t3 ^ 11u;
+  const uint32_t b = seed | 1u;
+  for (int i = 0; i < kProbeIters; i++) {
+    asm volatile(
+        "mad.lo.u32 %0, %8, %12, %0;\n\t"
+        "mad.hi.u32 %1, %8, %12, %1;\n\t"
+        "mad.lo.u32 %2, %9, %12, %2;\n\t"
+        "mad.hi.u32 %3, %9, %12, %3;\n\t"
+        "mad.lo.u32 %4, %10, %12, %4;\n\t"
+        "mad.hi.u32 %5, %10, %12, %5;\n\t"
+        "mad.lo.u32 %6, %11, %12, %6;\n\t"
+        "mad.hi.u32 %7, %11, %12, %7;\n\t"
+        "mad.hi.u32 %0, %9, %12, %0;\n\t"
+        "mad.lo.u32 %1, %9, %12, %1;\n\t"
+        "mad.hi.u32 %2, %10, %12, %2;\n\t"
+        "mad.lo.u32 %3, %10, %12, %3;\n\t"
+        "mad.hi.u32 %4, %11, %12, %4;\n\t"
+        "mad.lo.u32 %5, %11, %12, %5;\n\t"
+        "mad.hi.u32 %6, %8, %12, %6;\n\t"
+        "mad.lo.u32 %7, %8, %12, %7;"
+        : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7)
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b));
+  }
+  const uint32_t x = t0 ^ t1 ^ t2 ^ t3 ^ t4 ^ t5 ^ t6 ^ t7;
+  if (x == 0x12345678u) out[0] = x;
 }
 }  // namespace
 
@@ -96,7 +131,7 @@ void Profiler::collect(double* ms, double* launches, double* units) {
   recs.clear();
 }
 
-double imad_probe(cudaStream_t st) {
+double imad_probe(cudaStream_t st, int kind) {
   int dev = 0, sms = 0;
   ZK_CUDA(cudaGetDevice(&dev));
   ZK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -106,12 +141,18 @@ double imad_probe(cudaStream_t st) {
   cudaEvent_t a, b;
   ZK_CUDA(cudaEventCreate(&a));
   ZK_CUDA(cudaEventCreate(&b));
-  k_imad_probe<<<blocks, threads, 0, st>>>(1u, out.as<uint32_t>());  // warm-up
+  auto launch = [&](uint32_t seed) {
+    if (kind == 1)
+      k_imad_probe_free<<<blocks, threads, 0, st>>>(seed, out.as<uint32_t>());
+    else
+      k_imad_probe<<<blocks, threads, 0, st>>>(seed, out.as<uint32_t>());
+  };
+  launch(1u);  // warm-up
   count_launch(1);
   float best = 1e30f;
   for (int rep = 0; rep < 5; rep++) {
     ZK_CUDA(cudaEventRecord(a, st));
-    k_imad_probe<<<blocks, threads, 0, st>>>(3u + rep, out.as<uint32_t>());
+    launch(3u + rep);
     count_launch(1);
     ZK_CUDA(cudaEventRecord(b, st));
     ZK_CUDA(cudaEventSynchronize(b));

@@ -57,6 +57,9 @@ struct ProfScope {  // brackets one launch when profiling is on
 
 // Carry-chain IMAD throughput of the device (mad.lo.cc / madc.hi.cc pairs, as
 // in the field multiplication), in 10^12 32-bit multiply-adds per second.
-double imad_probe(cudaStream_t st);
+// Measured integer multiply-add throughput of the device in 10^12 ops/s at
+// full occupancy: kind 0 = carry chains (mad.lo.cc / madc.hi.cc, the field
+// products' mix), kind 1 = independent mad.lo / mad.hi streams (no carry).
+double imad_probe(cudaStream_t st, int kind = 0);
 
 }  // namespace zk

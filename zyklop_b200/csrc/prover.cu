@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "field.cuh"
@@ -442,7 +443,13 @@ void ws_pipeline(zk_circuit* c, ProveWs& ws, bool blind, ProveIntermediates* dbg
   }
   hpoly(ctx->ntt, ws.aw.as<uint64_t>(), ws.bw.as<uint64_t>(), ws.cw.as<uint64_t>(), c->log_n,
         ws.h.as<uint64_t>(), s0);
-  if (dbg && dbg->h) ZK_CUDA(cudaMemcpyAsync(dbg->h, ws.h.ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
+  if (dbg) {
+    // the H pipeline leaves the coset evaluations of A, B and C in aw, bw, cw
+    const std::pair<uint64_t*, const DeviceBuffer*> outs[] = {
+        {dbg->h, &ws.h}, {dbg->ea, &ws.aw}, {dbg->eb, &ws.bw}, {dbg->ec, &ws.cw}};
+    for (const auto& o : outs)
+      if (o.first) ZK_CUDA(cudaMemcpyAsync(o.first, o.second->ptr, 32 * n, cudaMemcpyDeviceToHost, s0));
+  }
   ws_msm(c, ws, 0, false, c->pts_h, c->tab_h, ws.h.as<uint64_t>(), n, nullptr,
          merge ? &ws.merge_c : nullptr);
   for (int i = 1; i < (blind ? 5 : 4); i++) ZK_CUDA(cudaStreamWaitEvent(s0, ws.ev_done[i], 0));
@@ -512,14 +519,22 @@ void ws_launch(zk_circuit* c, ProveWs& ws, bool blind, bool use_graph, ProveInte
 
 // Waits for the device work, combines the MSM results, applies blinding.
 void ws_finish(zk_circuit* c, ProveWs& ws, bool blind, const uint64_t* r, const uint64_t* s,
-               uint64_t proof[32]) {
+               uint64_t proof[32], ProveIntermediates* dbg = nullptr) {
   ZK_CUDA(cudaEventSynchronize(ws.ev_all));
   uint64_t pa[8], pb[16], pc[8], ph[8], pb1[8];
-  msm_g1_combine(ws.win[1].ptr, ws.res[1], pa);
-  msm_g2_combine(ws.win[2].ptr, ws.res[2], pb);
-  msm_g1_combine(ws.win[3].ptr, ws.res[3], pc);
-  msm_g1_combine(ws.win[0].ptr, ws.res[0], ph);
+  int inf[4];
+  inf[0] = msm_g1_combine(ws.win[1].ptr, ws.res[1], pa);
+  inf[1] = msm_g2_combine(ws.win[2].ptr, ws.res[2], pb);
+  inf[2] = msm_g1_combine(ws.win[3].ptr, ws.res[3], pc);
+  inf[3] = msm_g1_combine(ws.win[0].ptr, ws.res[0], ph);
   if (blind) msm_g1_combine(ws.win[4].ptr, ws.res[4], pb1);
+  if (dbg) {
+    memcpy(dbg->msm_a, pa, sizeof pa);
+    memcpy(dbg->msm_b2, pb, sizeof pb);
+    memcpy(dbg->msm_c, pc, sizeof pc);
+    memcpy(dbg->msm_h, ph, sizeof ph);
+    memcpy(dbg->inf, inf, sizeof inf);
+  }
   assemble_proof(c, pa, pb, pc, ph, blind ? pb1 : nullptr, r, s, proof);
 }
 
@@ -630,7 +645,7 @@ void prove(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool on_dev
   ws_launch(c, ws, blind, ctx->use_graphs, dbg);
   ZK_CUDA(cudaEventRecord(ws.ev_all, ws.st[0]));
   ZK_CUDA(cudaStreamWaitEvent(ctx->stream, ws.ev_all, 0));
-  ws_finish(c, ws, blind, r, s, proof);
+  ws_finish(c, ws, blind, r, s, proof, dbg);
 }
 
 void prove_oneshot(zk_ctx* ctx, const BinFile& zkey, const uint64_t* witness, size_t n_witness,

@@ -63,6 +63,15 @@ struct ProveIntermediates {
   uint64_t* aw = nullptr;  // host, domain x 4 (Montgomery A.w)
   uint64_t* bw = nullptr;  // host, domain x 4 (Montgomery B.w)
   uint64_t* h = nullptr;   // host, domain x 4 (canonical h)
+  // host, domain x 4: A, B and C = A.B evaluated on the odd coset
+  // omega_2n^(2j+1) (Montgomery, natural order), the H pipeline's last NTT
+  uint64_t* ea = nullptr;
+  uint64_t* eb = nullptr;
+  uint64_t* ec = nullptr;
+  // filled when the proof finishes: each MSM's own result (affine
+  // Montgomery; A includes alpha1, B2 beta2) and whether it is infinity
+  uint64_t msm_a[8] = {}, msm_b2[16] = {}, msm_c[8] = {}, msm_h[8] = {};
+  int inf[4] = {};
 };
 
 // Builds fixed-base tables for every point set of the circuit (c_g1 / c_g2

@@ -1,6 +1,7 @@
 // Runtime plumbing (see runtime.hpp).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
 #include <string>
@@ -11,6 +12,8 @@ namespace zk {
 
 namespace {
 thread_local std::string g_last_error;
+// allocations the library has made in this process (zk_memory_stats)
+std::atomic<uint64_t> g_dev_allocs{0}, g_dev_alloc_bytes{0}, g_host_allocs{0};
 }
 
 void set_last_error(int code, const char* msg) {
@@ -71,6 +74,21 @@ DevPool* pool_of(int dev) {
 }
 }  // namespace
 
+void alloc_stats(uint64_t* dev_allocs, uint64_t* dev_bytes, uint64_t* host_allocs) {
+  *dev_allocs = g_dev_allocs.load();
+  *dev_bytes = g_dev_alloc_bytes.load();
+  *host_allocs = g_host_allocs.load();
+}
+
+bool pool_usage(int dev, uint64_t* reserved, uint64_t* used) {
+  *reserved = *used = 0;
+  DevPool* p = pool_of(dev);
+  if (!p) return false;
+  cudaMemPoolGetAttribute(p->pool, cudaMemPoolAttrReservedMemCurrent, reserved);
+  cudaMemPoolGetAttribute(p->pool, cudaMemPoolAttrUsedMemCurrent, used);
+  return true;
+}
+
 size_t device_free_bytes() {
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
@@ -118,6 +136,8 @@ void DeviceBuffer::ensure(size_t bytes) {
     throw Error(ZK_ENOMEM, buf);
   }
   cap = want;
+  g_dev_allocs++;
+  g_dev_alloc_bytes += want;
 }
 
 void DeviceBuffer::release() {
@@ -149,6 +169,7 @@ void PinnedBuffer::ensure(size_t bytes) {
     throw Error(ZK_ENOMEM, std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
   }
   cap = want;
+  g_host_allocs++;
 }
 
 void PinnedBuffer::release() {

@@ -53,6 +53,11 @@ void set_last_error(int code, const char* msg);
 // Free device memory on the current device, counting blocks the library's
 // pool holds for reuse.
 size_t device_free_bytes();
+// Device / pinned-host allocations the library has made in this process.
+void alloc_stats(uint64_t* dev_allocs, uint64_t* dev_bytes, uint64_t* host_allocs);
+// Reserved and used bytes of the library's memory pool on `dev` (false if
+// the device has no pool).
+bool pool_usage(int dev, uint64_t* reserved, uint64_t* used);
 // Returns the pool's unused blocks on the current device to the driver.
 void release_cached_memory();
 
