@@ -95,6 +95,8 @@ def parse_args():
     p.add_argument("--config2-steps", type=int, default=10)
     p.add_argument("--parity-only", action="store_true",
                    help="(--impl reference) write the reference outputs without timing")
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the comparison with the reference build's outputs")
     return p.parse_args()
 
 
@@ -785,18 +787,28 @@ def pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
 
-def run_batched(args, dist, ctx, L):
-    """64 independent proofs over 8 seeded circuits with log-uniform sizes in
-    [2^14, 2^20] (circom-like witnesses, 1-4 nonzeros per row), all circuits
-    resident with fixed-base tables: zk_prove_batch (several proofs in flight,
-    CUDA-graph replay of each circuit's pipeline) against the same 64 proofs
-    one at a time through zk_prove, and through the one-shot file call."""
+def config3_sizes(n_circuits=8, seed=3):
+    """Circuit sizes (log2) of the batched workload: log-uniform in
+    [2^14, 2^20] with both ends present (the first two circuits are 2^14 and
+    2^20, the others drawn)."""
+    rng = np.random.default_rng(seed)
+    return [14, 20] + [int(round(x)) for x in rng.uniform(14, 20, n_circuits - 2)]
+
+
+def run_batched(args, dist, ctx, L, logs=None, n_proofs=None, seed=3, label="config3"):
+    """Independent proofs over seeded circuits (circom-like witnesses, 1-4
+    nonzeros per row), all circuits resident with fixed-base tables:
+    zk_prove_batch (in-flight pipelines with CUDA-graph replay, and fused
+    groups over multi-instance MSM chains) against the same proofs one at a
+    time through zk_prove, and through the one-shot file call.  Default:
+    config 3, 64 proofs over 8 circuits of log-uniform size in [2^14, 2^20]."""
     import torch
     from zyklop_b200 import api
     from zyklop_b200._lib import check
-    rng = np.random.default_rng(3)
-    logs = [int(round(x)) for x in rng.uniform(14, 20, 8)]
-    jobs = [int(j) for j in rng.integers(0, 8, args.batch_proofs)]
+    rng = np.random.default_rng(seed)
+    logs = logs or config3_sizes()
+    n_proofs = n_proofs or args.batch_proofs
+    jobs = [int(j) for j in rng.integers(0, len(logs), n_proofs)]
     files = [synth_cached(args, dist, lg, "circom", 100 + k) for k, lg in enumerate(logs)]
     t_tune = time.perf_counter()
     tuned = autotune_sizes(args, api, ctx, sorted(set(logs)), api.SKEWED)
@@ -859,8 +871,8 @@ def run_batched(args, dist, ctx, L):
         c.close()
     n = len(jobs)
     return {
-        "workload": f"{n} proofs, 8 circuits of 2^{min(logs)}..2^{max(logs)} constraints "
-                    f"(log-uniform, sizes {sorted(logs)}), circom-like witnesses",
+        "workload": f"{label}: {n} proofs, {len(logs)} circuits of 2^{min(logs)}..2^{max(logs)} "
+                    f"constraints (sizes {sorted(logs)}), circom-like witnesses",
         "batched_proofs_per_s": n / (batch_ms / 1e3),
         "plain_proofs_per_s": n / (plain_ms / 1e3),
         "speedup_vs_plain": plain_ms / batch_ms,
@@ -1208,6 +1220,9 @@ def main():
             line["config2"] = c2
         if dist.world == 1 and args.batch_proofs > 0:
             line["batched"] = run_batched(args, dist, ctx, lib_handle())
+            # the same comparison at 2^20 alone: 16 proofs over two 2^20 circuits
+            line["batched"]["at_2^20"] = run_batched(args, dist, ctx, lib_handle(), logs=[20, 20],
+                                                     n_proofs=16, seed=5, label="2^20 only")
         if dist.world == 1 and args.serve_seconds > 0:
             line["serving"] = run_serving(args, dist, ctx, lib_handle())
         if dist.world == 1 and (args.prim_g1 or args.prim_g2 or args.prim_ntt):
@@ -1221,7 +1236,7 @@ def main():
         lib_handle().zk_ctx_destroy(ctx)
         if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(*files)
-        if dist.rank == 0 and dist.world == 1:
+        if dist.rank == 0 and dist.world == 1 and not args.no_parity:
             ref, source = reference_outputs(args)
             line["parity_vs_reference"] = parity_report(mine_out, ref, source)
             if ref and "config2" in line and "config2_value" in ref:

@@ -44,7 +44,11 @@ const char* zk_last_error(void);
 /* A context owns one CUDA stream, the device scratch arena and the cached NTT
  * twiddle tables for one device.  Calls on one context are serialized; use
  * one context per host thread for concurrency.  Passing ctx = NULL to any
- * entry point uses a per-device default context (current device).
+ * entry point uses a per-device default context (current device).  A
+ * context's own stream is a blocking stream: its work starts after work the
+ * caller queued on the legacy default stream (the stream the reference uses
+ * for everything), so device buffers written there are ready; use
+ * zk_ctx_set_stream to run on another stream instead.
  * Replaces the reference's global state (g_ntt_* statics,
  * include/ntt_bn254.cuh:50-53; implicit device 0 and legacy stream). */
 int zk_ctx_create(int device, zk_ctx** out);

@@ -14,7 +14,7 @@ import json
 import os
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ZK_REFERENCE_DIR", "/root/reference")
 UNIT = os.path.join(REF, "test", "unit")
 OUT = os.path.dirname(os.path.abspath(__file__))
 

@@ -220,17 +220,23 @@ void fused_launch(zk_ctx* ctx, FusedWs& f, Group& g, const uint64_t* const* wits
 void fused_finish(FusedWs& f, const Group& g, bool blind, const uint64_t* rs, const uint64_t* ss,
                   uint64_t* proofs) {
   ZK_CUDA(cudaEventSynchronize(f.ev_done));
-  for (size_t k = 0; k < g.jobs.size(); k++) {
+  const size_t nj = g.jobs.size();
+  std::vector<ProofXyzz> px(nj);
+  std::vector<uint64_t*> out(nj);
+  for (size_t k = 0; k < nj; k++) {
     const size_t i = g.jobs[k].idx, b = k * g.per_job;
-    uint64_t pa[8], pb[16], pc[8], ph[8], pb1[8];
-    msm_g1_combine_inst(f.win1w.ptr, g.rw, (int)b, pa);
-    msm_g1_combine_inst(f.win1w.ptr, g.rw, (int)b + 1, pc);
-    if (blind) msm_g1_combine_inst(f.win1w.ptr, g.rw, (int)b + 2, pb1);
-    msm_g1_combine_inst(f.winh.ptr, g.rh, (int)k, ph);
-    msm_g2_combine_inst(f.win2.ptr, g.r2, (int)k, pb);
-    assemble_proof(g.jobs[k].c, pa, pb, pc, ph, blind ? pb1 : nullptr,
-                   blind ? rs + 4 * i : nullptr, blind ? ss + 4 * i : nullptr, proofs + 32 * i);
+    const auto a = msm_g1_combine_xyzz(f.win1w.ptr, g.rw, (int)b);
+    const auto c = msm_g1_combine_xyzz(f.win1w.ptr, g.rw, (int)b + 1);
+    const auto h = msm_g1_combine_xyzz(f.winh.ptr, g.rh, (int)k);
+    const auto b2 = msm_g2_combine_xyzz(f.win2.ptr, g.r2, (int)k);
+    host::Xyzz<host::Fp> b1;
+    if (blind) b1 = msm_g1_combine_xyzz(f.win1w.ptr, g.rw, (int)b + 2);
+    px[k] = assemble_proof(g.jobs[k].c, a, b2, c.add(h), blind ? &b1 : nullptr,
+                           blind ? rs + 4 * i : nullptr, blind ? ss + 4 * i : nullptr);
+    out[k] = proofs + 32 * i;
   }
+  // every proof of the group made affine with one shared inversion
+  proofs_to_affine(px.data(), nj, out.data());
 }
 
 }  // namespace

@@ -50,7 +50,9 @@ zk_ctx* default_ctx() {
     zk_ctx* c = new zk_ctx();
     c->device = dev;
     c->is_default = true;
-    ZK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    // a blocking stream: ordered after the caller's work on the legacy
+    // default stream, which is where the reference runs everything
+    ZK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault));
     g_defaults[dev] = c;
   }
   return g_defaults[dev];
@@ -80,7 +82,7 @@ int zk_ctx_create(int device, zk_ctx** out) {
   ZK_CUDA(cudaSetDevice(device));
   zk_ctx* c = new zk_ctx();
   c->device = device;
-  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault);
   if (e != cudaSuccess) {
     delete c;
     throw_cuda(e, "cudaStreamCreateWithFlags", __FILE__, __LINE__);

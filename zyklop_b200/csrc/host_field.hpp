@@ -190,6 +190,12 @@ struct Xyzz {
     if (ax.is_zero() && ay.is_zero()) return inf();
     return {ax, ay, T::one(), T::one()};
   }
+  // affine coordinates given zzzi = 1 / ZZZ (not at infinity)
+  void to_affine_with(const T& zzzi, T& ax, T& ay) const {
+    const T zi = zzzi * zz;  // ZZ / ZZZ = 1 / Z
+    ax = x * zi.sqr();
+    ay = y * zzzi;
+  }
   // returns true for the point at infinity; (0,0) written then
   bool to_affine(T& ax, T& ay) const {
     if (is_inf()) {
@@ -205,6 +211,57 @@ struct Xyzz {
     return false;
   }
 };
+
+// Inverts every nonzero v[i] in place with one field inversion in all
+// (Montgomery's simultaneous-inversion trick: prefix products, one inverse,
+// three products per value on the way back); zeros stay zero.
+inline void batch_inv(Fp* v, size_t n) {
+  if (!n) return;
+  Fp* pre = new Fp[n];
+  Fp acc = Fp::one();
+  for (size_t i = 0; i < n; i++) {
+    pre[i] = acc;
+    if (!v[i].is_zero()) acc = acc * v[i];
+  }
+  Fp inv = acc.inv();
+  for (size_t i = n; i-- > 0;) {
+    if (v[i].is_zero()) continue;
+    const Fp vi = v[i];
+    v[i] = inv * pre[i];
+    inv = inv * vi;
+  }
+  delete[] pre;
+}
+
+// Affine forms of G1 and G2 XYZZ points with a single shared inversion: the
+// Fp inverses of every G1 point's ZZZ and of every G2 point's ZZZ norm
+// (1 / z = conj(z) / (z0^2 + z1^2) in Fp2) come from one batch_inv.  Points
+// at infinity give (0, 0) and inf[k] = true.  The reference inverts once per
+// point (jacToAff with its BY inversion, include/fp_bn254.cuh:720-773).
+inline void batch_to_affine(const Xyzz<Fp>* g1, size_t n1, Fp* x1, Fp* y1, bool* inf1,
+                            const Xyzz<Fp2>* g2, size_t n2, Fp2* x2, Fp2* y2, bool* inf2) {
+  Fp* d = new Fp[n1 + n2];
+  for (size_t i = 0; i < n1; i++) d[i] = g1[i].is_inf() ? Fp::zero() : g1[i].zzz;
+  for (size_t i = 0; i < n2; i++)
+    d[n1 + i] = g2[i].is_inf() ? Fp::zero() : g2[i].zzz.c0.sqr() + g2[i].zzz.c1.sqr();
+  batch_inv(d, n1 + n2);
+  for (size_t i = 0; i < n1; i++) {
+    inf1[i] = g1[i].is_inf();
+    if (inf1[i]) x1[i] = y1[i] = Fp::zero();
+    else g1[i].to_affine_with(d[i], x1[i], y1[i]);
+  }
+  for (size_t i = 0; i < n2; i++) {
+    inf2[i] = g2[i].is_inf();
+    if (inf2[i]) {
+      x2[i] = y2[i] = Fp2::zero();
+    } else {
+      const Fp n = d[n1 + i];
+      const Fp2 zi{g2[i].zzz.c0 * n, -(g2[i].zzz.c1 * n)};
+      g2[i].to_affine_with(zi, x2[i], y2[i]);
+    }
+  }
+  delete[] d;
+}
 
 }  // namespace host
 }  // namespace zk

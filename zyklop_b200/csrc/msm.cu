@@ -1011,31 +1011,49 @@ bool msm_g2_combine_inst(const void* h_data, const MsmResult& r, int inst, uint6
   return msm_g2_combine(buf, one, out);
 }
 
-bool msm_g1_combine(const void* h_data, const MsmResult& r, uint64_t out[8]) {
+host::Xyzz<host::Fp> msm_g1_combine_xyzz(const void* h_data, const MsmResult& r, int inst) {
   using P = host::Xyzz<host::Fp>;
-  const P acc = combine<host::Fp>(reinterpret_cast<const uint8_t*>(h_data), r, 128,
-                                  [](const uint8_t* p) {
-                                    const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
-                                    return P{fp_from_words(q), fp_from_words(q + 8),
-                                             fp_from_words(q + 16), fp_from_words(q + 24)};
-                                  });
+  alignas(16) uint8_t buf[256];
+  MsmResult one = r;
+  if (inst >= 0) {
+    one = gather_instance(h_data, r, inst, 128, buf);
+    h_data = buf;
+  }
+  return combine<host::Fp>(reinterpret_cast<const uint8_t*>(h_data), one, 128,
+                           [](const uint8_t* p) {
+                             const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
+                             return P{fp_from_words(q), fp_from_words(q + 8), fp_from_words(q + 16),
+                                      fp_from_words(q + 24)};
+                           });
+}
+
+host::Xyzz<host::Fp2> msm_g2_combine_xyzz(const void* h_data, const MsmResult& r, int inst) {
+  using P = host::Xyzz<host::Fp2>;
+  alignas(16) uint8_t buf[512];
+  MsmResult one = r;
+  if (inst >= 0) {
+    one = gather_instance(h_data, r, inst, 256, buf);
+    h_data = buf;
+  }
+  return combine<host::Fp2>(reinterpret_cast<const uint8_t*>(h_data), one, 256,
+                            [](const uint8_t* p) {
+                              const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
+                              return P{fp2_from_words(q), fp2_from_words(q + 16),
+                                       fp2_from_words(q + 32), fp2_from_words(q + 48)};
+                            });
+}
+
+bool msm_g1_combine(const void* h_data, const MsmResult& r, uint64_t out[8]) {
   host::Fp x, y;
-  const bool inf = acc.to_affine(x, y);
+  const bool inf = msm_g1_combine_xyzz(h_data, r).to_affine(x, y);
   memcpy(out, x.v, 32);
   memcpy(out + 4, y.v, 32);
   return inf;
 }
 
 bool msm_g2_combine(const void* h_data, const MsmResult& r, uint64_t out[16]) {
-  using P = host::Xyzz<host::Fp2>;
-  const P acc = combine<host::Fp2>(reinterpret_cast<const uint8_t*>(h_data), r, 256,
-                                   [](const uint8_t* p) {
-                                     const uint32_t* q = reinterpret_cast<const uint32_t*>(p);
-                                     return P{fp2_from_words(q), fp2_from_words(q + 16),
-                                              fp2_from_words(q + 32), fp2_from_words(q + 48)};
-                                   });
   host::Fp2 x, y;
-  const bool inf = acc.to_affine(x, y);
+  const bool inf = msm_g2_combine_xyzz(h_data, r).to_affine(x, y);
   memcpy(out, x.c0.v, 32);
   memcpy(out + 4, x.c1.v, 32);
   memcpy(out + 8, y.c0.v, 32);

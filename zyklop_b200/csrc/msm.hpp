@@ -28,6 +28,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "host_field.hpp"
 #include "runtime.hpp"
 
 namespace zk {
@@ -132,6 +133,10 @@ MsmResult msm_enqueue_fixed_multi(bool g2, int inst, const void* const* tables,
 
 // Host combination of an MSM result (r.bytes copied from r.d_data) into an
 // affine Montgomery point.  Returns true for the point at infinity.
+// The same sums left in XYZZ coordinates (inst >= 0: that instance of a
+// multi-instance result), for callers that batch the affine conversions.
+host::Xyzz<host::Fp> msm_g1_combine_xyzz(const void* h_data, const MsmResult& r, int inst = -1);
+host::Xyzz<host::Fp2> msm_g2_combine_xyzz(const void* h_data, const MsmResult& r, int inst = -1);
 bool msm_g1_combine(const void* h_data, const MsmResult& r, uint64_t out[8]);
 bool msm_g2_combine(const void* h_data, const MsmResult& r, uint64_t out[16]);
 bool msm_g1_combine_inst(const void* h_data, const MsmResult& r, int inst, uint64_t out[8]);

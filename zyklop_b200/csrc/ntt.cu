@@ -61,11 +61,54 @@ struct HArgs {
   fr_t* h[kMaxHBatch];
 };
 
-// One pass: radix-2 stages on global index bits [lo, lo + k) for every
+// One pass: the stages on global index bits [lo, lo + k) for every
 // sub-transform, in shared memory.  DIF runs the bits high -> low with
 // butterflies (u + v, (u - v) w); DIT runs low -> high with (u + v w, u - v w).
 // In both, the butterfly on bit b of pair (i, i + 2^b) uses
-// w^((i mod 2^b) << (L - 1 - b)).
+// w^((i mod 2^b) << (L - 1 - b)).  Stages go two at a time where they can
+// (radix 4: a thread loads a quad of elements, runs both stages in registers
+// and stores it back, one shared-memory round trip and one barrier for two
+// stages); the butterflies of global bit 0 have w = 1 and skip the product.
+struct NttSlots {
+  const uint32_t* sm;
+  int tile;
+};
+
+__device__ __forceinline__ fr_t sm_load(const uint32_t* sm, int tile, int slot) {
+  fr_t x;
+#pragma unroll
+  for (int q = 0; q < 8; q++) x.v[q] = sm[q * tile + slot];
+  return x;
+}
+__device__ __forceinline__ void sm_store(uint32_t* sm, int tile, int slot, const fr_t& x) {
+#pragma unroll
+  for (int q = 0; q < 8; q++) sm[q * tile + slot] = x.v[q];
+}
+
+// twiddle of the butterfly on local bit `bit` whose pair starts at local
+// index j (only j mod 2^bit matters) in group g of the block
+__device__ __forceinline__ fr_t ntt_twiddle(const fr_t* __restrict__ tw, int tw_shift, int L, int lo,
+                                            int bit, int j, size_t gid) {
+  const size_t lomask = (size_t(1) << lo) - 1;
+  const size_t imod = ((size_t)(j & ((1 << bit) - 1)) << lo) | (gid & lomask);
+  return fe_ldg<FrCfg>(tw, (imod << (L - 1 - (lo + bit))) << tw_shift);
+}
+
+template <bool DIT>
+__device__ __forceinline__ void butterfly(fr_t& u, fr_t& v, const fr_t& w, bool trivial) {
+  if (DIT) {
+    if (!trivial) v = fe_mul_inline(v, w);
+    const fr_t a = u + v;
+    v = u - v;
+    u = a;
+  } else {
+    const fr_t a = u + v;
+    v = u - v;
+    if (!trivial) v = fe_mul_inline(v, w);
+    u = a;
+  }
+}
+
 template <bool DIT>
 __global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const fr_t* __restrict__ tw,
                                                            int tw_shift, int L, int lo, int k,
@@ -88,45 +131,67 @@ __global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const 
     }
     const size_t gid = gid0 + g;
     const size_t idx = ((gid >> lo) << (lo + k)) | ((size_t)j << lo) | (gid & lomask);
-    const fr_t x = fe_load<FrCfg>(in, idx);
-    const int slot = (j << log_g) | g;
-#pragma unroll
-    for (int w = 0; w < 8; w++) sm[w * tile + slot] = x.v[w];
+    sm_store(sm, tile, (j << log_g) | g, fe_load<FrCfg>(in, idx));
   }
   __syncthreads();
-  for (int st = 0; st < k; st++) {
-    const int bit = DIT ? st : (k - 1 - st);
-    const int gbit = lo + bit;
-    for (int bf = threadIdx.x; bf < tile / 2; bf += blockDim.x) {
-      const int g = bf & (G - 1);
-      const int jb = bf >> log_g;
-      const int jlo = jb & ((1 << bit) - 1), jhi = jb >> bit;
-      const int j0 = (jhi << (bit + 1)) | jlo;
-      const int s0 = (j0 << log_g) | g;
-      const int s1 = s0 | (1 << (bit + log_g));
-      const size_t gid = gid0 + g;
-      const size_t imod = ((size_t)jlo << lo) | (gid & lomask);
-      const fr_t w = fe_ldg<FrCfg>(tw, (imod << (L - 1 - gbit)) << tw_shift);
-      fr_t u, v;
-#pragma unroll
-      for (int q = 0; q < 8; q++) {
-        u.v[q] = sm[q * tile + s0];
-        v.v[q] = sm[q * tile + s1];
+  for (int st = 0; st < k;) {
+    if (st + 1 < k) {
+      // two stages: DIT bits (b, b + 1) low first, DIF bits (b + 1, b) high first
+      const int b = DIT ? st : (k - 2 - st);
+      for (int qd = threadIdx.x; qd < tile / 4; qd += blockDim.x) {
+        const int g = qd & (G - 1);
+        const int jq = qd >> log_g;  // quad index over the k - 2 other bits
+        const int jlo = jq & ((1 << b) - 1), jhi = jq >> b;
+        const int j0 = (jhi << (b + 2)) | jlo;
+        const int s00 = (j0 << log_g) | g;
+        const int s01 = s00 | (1 << (b + log_g));
+        const int s10 = s00 | (2 << (b + log_g));
+        const int s11 = s01 | s10;
+        const size_t gid = gid0 + g;
+        fr_t x00 = sm_load(sm, tile, s00), x01 = sm_load(sm, tile, s01);
+        fr_t x10 = sm_load(sm, tile, s10), x11 = sm_load(sm, tile, s11);
+        const bool triv = lo + b == 0;  // bit 0 of the transform: w = 1
+        // twiddles are loaded right before their butterflies (fewer live registers)
+        auto low = [&] {
+          const fr_t w = triv ? fr_t{} : ntt_twiddle(tw, tw_shift, L, lo, b, j0, gid);
+          butterfly<DIT>(x00, x01, w, triv);
+          butterfly<DIT>(x10, x11, w, triv);
+        };
+        auto high = [&] {
+          butterfly<DIT>(x00, x10, ntt_twiddle(tw, tw_shift, L, lo, b + 1, j0, gid), false);
+          butterfly<DIT>(x01, x11, ntt_twiddle(tw, tw_shift, L, lo, b + 1, j0 | (1 << b), gid),
+                         false);
+        };
+        if (DIT) {
+          low();
+          high();
+        } else {
+          high();
+          low();
+        }
+        sm_store(sm, tile, s00, x00);
+        sm_store(sm, tile, s01, x01);
+        sm_store(sm, tile, s10, x10);
+        sm_store(sm, tile, s11, x11);
       }
-      fr_t a, b;
-      if (DIT) {
-        v = fe_mul_inline(v, w);
-        a = u + v;
-        b = u - v;
-      } else {
-        a = u + v;
-        b = fe_mul_inline(u - v, w);
+      st += 2;
+    } else {
+      const int bit = DIT ? st : (k - 1 - st);
+      for (int bf = threadIdx.x; bf < tile / 2; bf += blockDim.x) {
+        const int g = bf & (G - 1);
+        const int jb = bf >> log_g;
+        const int jlo = jb & ((1 << bit) - 1), jhi = jb >> bit;
+        const int j0 = (jhi << (bit + 1)) | jlo;
+        const int s0 = (j0 << log_g) | g;
+        const int s1 = s0 | (1 << (bit + log_g));
+        const bool triv = lo + bit == 0;
+        const fr_t w = triv ? fr_t{} : ntt_twiddle(tw, tw_shift, L, lo, bit, j0, gid0 + g);
+        fr_t u = sm_load(sm, tile, s0), v = sm_load(sm, tile, s1);
+        butterfly<DIT>(u, v, w, triv);
+        sm_store(sm, tile, s0, u);
+        sm_store(sm, tile, s1, v);
       }
-#pragma unroll
-      for (int q = 0; q < 8; q++) {
-        sm[q * tile + s0] = a.v[q];
-        sm[q * tile + s1] = b.v[q];
-      }
+      st += 1;
     }
     __syncthreads();
   }
@@ -141,11 +206,7 @@ __global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const 
     }
     const size_t gid = gid0 + g;
     const size_t idx = ((gid >> lo) << (lo + k)) | ((size_t)j << lo) | (gid & lomask);
-    const int slot = (j << log_g) | g;
-    fr_t x;
-#pragma unroll
-    for (int w = 0; w < 8; w++) x.v[w] = sm[w * tile + slot];
-    fe_store(out, idx, x);
+    fe_store(out, idx, sm_load(sm, tile, (j << log_g) | g));
   }
 }
 

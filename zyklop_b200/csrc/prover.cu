@@ -84,19 +84,27 @@ host::Fp fp(const uint64_t* p) { return host::Fp::from_raw(p); }
 host::Fp2 fp2(const uint64_t* p) { return host::Fp2{fp(p), fp(p + 4)}; }
 G1 g1_aff(const uint64_t* p) { return G1::from_affine(fp(p), fp(p + 4)); }
 G2 g2_aff(const uint64_t* p) { return G2::from_affine(fp2(p), fp2(p + 8)); }
-void g1_out(const G1& g, uint64_t* out) {
-  host::Fp x, y;
-  g.to_affine(x, y);
+void put_g1(const host::Fp& x, const host::Fp& y, uint64_t* out) {
   memcpy(out, x.v, 32);
   memcpy(out + 4, y.v, 32);
 }
-void g2_out(const G2& g, uint64_t* out) {
-  host::Fp2 x, y;
-  g.to_affine(x, y);
+void put_g2(const host::Fp2& x, const host::Fp2& y, uint64_t* out) {
   memcpy(out, x.c0.v, 32);
   memcpy(out + 4, x.c1.v, 32);
   memcpy(out + 8, y.c0.v, 32);
   memcpy(out + 12, y.c1.v, 32);
+}
+int g1_out(const G1& g, uint64_t* out) {
+  host::Fp x, y;
+  const bool inf = g.to_affine(x, y);
+  put_g1(x, y, out);
+  return inf ? 1 : 0;
+}
+int g2_out(const G2& g, uint64_t* out) {
+  host::Fp2 x, y;
+  const bool inf = g.to_affine(x, y);
+  put_g2(x, y, out);
+  return inf ? 1 : 0;
 }
 template <class P>
 P mul(const P& p, const uint64_t* k) {
@@ -521,21 +529,22 @@ void ws_launch(zk_circuit* c, ProveWs& ws, bool blind, bool use_graph, ProveInte
 void ws_finish(zk_circuit* c, ProveWs& ws, bool blind, const uint64_t* r, const uint64_t* s,
                uint64_t proof[32], ProveIntermediates* dbg = nullptr) {
   ZK_CUDA(cudaEventSynchronize(ws.ev_all));
-  uint64_t pa[8], pb[16], pc[8], ph[8], pb1[8];
-  int inf[4];
-  inf[0] = msm_g1_combine(ws.win[1].ptr, ws.res[1], pa);
-  inf[1] = msm_g2_combine(ws.win[2].ptr, ws.res[2], pb);
-  inf[2] = msm_g1_combine(ws.win[3].ptr, ws.res[3], pc);
-  inf[3] = msm_g1_combine(ws.win[0].ptr, ws.res[0], ph);
-  if (blind) msm_g1_combine(ws.win[4].ptr, ws.res[4], pb1);
+  const G1 a = msm_g1_combine_xyzz(ws.win[1].ptr, ws.res[1]);
+  const G2 b = msm_g2_combine_xyzz(ws.win[2].ptr, ws.res[2]);
+  const G1 cc = msm_g1_combine_xyzz(ws.win[3].ptr, ws.res[3]);
+  const G1 h = msm_g1_combine_xyzz(ws.win[0].ptr, ws.res[0]);
+  G1 b1;
+  if (blind) b1 = msm_g1_combine_xyzz(ws.win[4].ptr, ws.res[4]);
   if (dbg) {
-    memcpy(dbg->msm_a, pa, sizeof pa);
-    memcpy(dbg->msm_b2, pb, sizeof pb);
-    memcpy(dbg->msm_c, pc, sizeof pc);
-    memcpy(dbg->msm_h, ph, sizeof ph);
-    memcpy(dbg->inf, inf, sizeof inf);
+    // each MSM's own affine result (the traced path only)
+    dbg->inf[0] = g1_out(a, dbg->msm_a);
+    dbg->inf[1] = g2_out(b, dbg->msm_b2);
+    dbg->inf[2] = g1_out(cc, dbg->msm_c);
+    dbg->inf[3] = g1_out(h, dbg->msm_h);
   }
-  assemble_proof(c, pa, pb, pc, ph, blind ? pb1 : nullptr, r, s, proof);
+  const ProofXyzz p = assemble_proof(c, a, b, cc.add(h), blind ? &b1 : nullptr, r, s);
+  uint64_t* out = proof;
+  proofs_to_affine(&p, 1, &out);
 }
 
 }  // namespace
@@ -555,23 +564,39 @@ void spmv_enqueue(zk_circuit* c, const uint64_t* we, uint64_t* aw, uint64_t* bw,
   ZK_LAUNCHED();
 }
 
-void assemble_proof(const zk_circuit* c, const uint64_t pa[8], const uint64_t pb[16],
-                    const uint64_t pc[8], const uint64_t ph[8], const uint64_t* pb1,
-                    const uint64_t* r, const uint64_t* s, uint64_t proof[32]) {
-  G1 A = g1_aff(pa), Cc = g1_aff(pc).add(g1_aff(ph));
-  G2 B = g2_aff(pb);
-  if (pb1) {
+ProofXyzz assemble_proof(const zk_circuit* c, const G1& a, const G2& b, const G1& c_plus_h,
+                         const G1* b1, const uint64_t* r, const uint64_t* s) {
+  ProofXyzz p{a, c_plus_h, b};
+  if (b1) {
     const G1 d1 = g1_aff(c->delta1);
-    A = A.add(mul(d1, r));
-    B = B.add(mul(g2_aff(c->delta2), s));
-    const G1 B1 = g1_aff(pb1).add(mul(d1, s));
+    p.a = p.a.add(mul(d1, r));
+    p.b = p.b.add(mul(g2_aff(c->delta2), s));
+    const G1 B1 = b1->add(mul(d1, s));
     host::Fr rs = host::Fr::from_raw(r).to_mont() * host::Fr::from_raw(s).to_mont();
     const host::Fr nrs = (-rs).from_mont();
-    Cc = Cc.add(mul(A, s)).add(mul(B1, r)).add(mul(d1, nrs.v));
+    p.c = p.c.add(mul(p.a, s)).add(mul(B1, r)).add(mul(d1, nrs.v));
   }
-  g1_out(A, proof);
-  g2_out(B, proof + 8);
-  g1_out(Cc, proof + 24);
+  return p;
+}
+
+void proofs_to_affine(const ProofXyzz* p, size_t n, uint64_t* const* out) {
+  std::vector<G1> g1(2 * n);
+  std::vector<G2> g2(n);
+  for (size_t i = 0; i < n; i++) {
+    g1[2 * i] = p[i].a;
+    g1[2 * i + 1] = p[i].c;
+    g2[i] = p[i].b;
+  }
+  std::vector<host::Fp> x1(2 * n), y1(2 * n);
+  std::vector<host::Fp2> x2(n), y2(n);
+  std::unique_ptr<bool[]> inf1(new bool[2 * n]), inf2(new bool[n]);
+  host::batch_to_affine(g1.data(), 2 * n, x1.data(), y1.data(), inf1.get(), g2.data(), n,
+                        x2.data(), y2.data(), inf2.get());
+  for (size_t i = 0; i < n; i++) {
+    put_g1(x1[2 * i], y1[2 * i], out[i]);
+    put_g2(x2[i], y2[i], out[i] + 8);
+    put_g1(x1[2 * i + 1], y1[2 * i + 1], out[i] + 24);
+  }
 }
 
 void check_job(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool blind) {

@@ -117,11 +117,20 @@ void check_job(zk_circuit* c, const uint64_t* witness, size_t n_witness, bool bl
 void note_witness(zk_circuit* c, const uint64_t* witness, bool on_device);
 // A.w, B.w (Montgomery, domain entries each) from we = [1 || w] on `st`.
 void spmv_enqueue(zk_circuit* c, const uint64_t* we, uint64_t* aw, uint64_t* bw, cudaStream_t st);
-// pi_A, pi_B, pi_C from the MSM sums (affine Montgomery); pb1 (the B1 MSM),
-// r and s are null for the unblinded proof.
-void assemble_proof(const zk_circuit* c, const uint64_t pa[8], const uint64_t pb[16],
-                    const uint64_t pc[8], const uint64_t ph[8], const uint64_t* pb1,
-                    const uint64_t* r, const uint64_t* s, uint64_t proof[32]);
+// pi_A, pi_B, pi_C in XYZZ coordinates, before the affine conversion.
+struct ProofXyzz {
+  host::Xyzz<host::Fp> a, c;
+  host::Xyzz<host::Fp2> b;
+};
+// pi_A, pi_B, pi_C from the MSM sums: a = A (alpha1 included), b = B2
+// (beta2 included), c = the C part plus the H part; b1 (the B1 MSM), r and s
+// are null for the unblinded proof.
+ProofXyzz assemble_proof(const zk_circuit* c, const host::Xyzz<host::Fp>& a,
+                         const host::Xyzz<host::Fp2>& b, const host::Xyzz<host::Fp>& c_plus_h,
+                         const host::Xyzz<host::Fp>* b1, const uint64_t* r, const uint64_t* s);
+// Affine proofs (pi_A[8], pi_B[16], pi_C[8] u64 Montgomery) of n assembled
+// proofs with one field inversion for all of them.
+void proofs_to_affine(const ProofXyzz* p, size_t n, uint64_t* const* out);
 
 uint64_t next_circuit_id();
 
