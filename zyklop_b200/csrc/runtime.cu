@@ -1,6 +1,8 @@
 // Runtime plumbing (see runtime.hpp).
 #include <cuda_runtime.h>
 
+#include <omp.h>
+
 #include <atomic>
 #include <cstdarg>
 #include <cstring>
@@ -183,6 +185,19 @@ Stager::~Stager() {
     if (e) cudaEventDestroy(e);
 }
 
+namespace {
+// host threads that copy into the pinned staging buffers: measured on the
+// pool's 16-core hosts, 16 threads keep the copy at the PCIe rate (587 MB in
+// 12 ms, the pinned-only DMA time) where 8 take 13-16 ms
+int stage_threads() {
+  static const int n = [] {
+    const int p = omp_get_num_procs();
+    return p < 1 ? 1 : (p > 16 ? 16 : p);
+  }();
+  return n;
+}
+}  // namespace
+
 void Stager::upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   if (!bytes) return;
   for (int i = 0; i < 2; i++) {
@@ -197,7 +212,8 @@ void Stager::upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
     ZK_CUDA(cudaEventSynchronize(ev[b]));  // previous DMA from this buffer is done
     char* p = buf[b].as<char>();
     const long parts = (long)((len + (size_t(1) << 20) - 1) >> 20);
-#pragma omp parallel for schedule(static) num_threads(8)
+    const int nt = stage_threads();
+#pragma omp parallel for schedule(static) num_threads(nt)
     for (long q = 0; q < parts; q++) {
       const size_t o = (size_t)q << 20;
       const size_t l = len - o < (size_t(1) << 20) ? len - o : (size_t(1) << 20);
