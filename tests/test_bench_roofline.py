@@ -18,11 +18,15 @@ def test_table_windows_from_flag_tuning_and_default():
 
 def test_issued_fraction_counts_records_and_issued_ops():
     # one G1 launch of 2^20 points in 4 ms, 13 records per point
-    r = bench.roofline_of("accum_g1", (4.0, 1, float(1 << 20)), 12.0, None, 13,
-                          {"carry_chain_probe": 12.0, "independent_mad_probe": 18.0})
+    variants = {"carry_chain_probe": 12.0, "independent_mad_probe": 18.0}
     conv = (1 << 20) * 176 * 264 / 4e-3 / 1e12
     issued = (1 << 20) * 13 * bench.ISSUED_IMAD_PER_RECORD["accum_g1"] / 4e-3 / 1e12
-    # the headline counts issued work; the convention is kept beside it
+    # the default headline is the fixed algorithmic work, issued beside it
+    r0 = bench.roofline_of("accum_g1", (4.0, 1, float(1 << 20)), 12.0, None, 13, variants)
+    assert r0["work"] == "convention" and abs(r0["frac"] - conv / 12.0) < 1e-12
+    assert abs(r0["issued"]["frac"] - issued / 12.0) < 1e-12
+    r = bench.roofline_of("accum_g1", (4.0, 1, float(1 << 20)), 12.0, None, 13, variants,
+                          headline="issued")
     assert r["work"] == "issued"
     assert abs(r["achieved"] - issued) < 1e-9 and abs(r["frac"] - issued / 12.0) < 1e-12
     assert abs(r["convention"]["achieved"] - conv) < 1e-9
