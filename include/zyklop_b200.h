@@ -245,17 +245,22 @@ int zk_prove_batch(zk_ctx* ctx, size_t count, zk_circuit* const* circuits,
                    const uint64_t* r, const uint64_t* s, uint64_t* proofs, int inflight);
 /* When on, each workspace captures a proof's device pipeline (about 60
  * kernels and copies across 5 streams) into a CUDA graph the first time it
- * proves a circuit and replays it afterwards.  Results are unchanged. */
+ * proves a circuit and replays it afterwards; in fused batches (mode 2),
+ * each group's device pipeline (its MSM chains, SpMVs and H pipelines) is
+ * captured the first time that group of jobs comes and replayed when it
+ * comes again.  Results are unchanged. */
 int zk_ctx_set_graphs(zk_ctx* ctx, int on);
 /* How zk_prove_batch runs: mode 1 = in-flight pipelines (up to `inflight`
  * proofs at once, each with its own workspace and streams); mode 2 = fused
  * groups: proofs over circuits with fixed-base tables (zk_circuit_precompute)
  * are grouped by table window bits, up to `group` per group, and each group
- * runs two multi-instance MSM launch chains (every job's G1 MSMs in one,
- * every job's B2 in the other) after per-job SpMV / H, with two groups
- * alternating so host combination overlaps GPU work; mode 0 (default) =
- * fused when every circuit has tables, else in-flight.  Results never
- * change. */
+ * runs three multi-instance MSM launch chains (every job's A and C, every
+ * job's B2, every job's H) whose bucket accumulation is a persistent kernel
+ * pulling (instance, bucket-range) tiles from a device work queue, per-job
+ * SpMVs, and every job's H pipeline (of any sizes) in one persistent launch
+ * pulling (job, step, tile) items from a device work queue; two groups
+ * alternate so host combination overlaps GPU work; mode 0 (default) = fused
+ * when every circuit has tables, else in-flight.  Results never change. */
 int zk_ctx_set_batch_mode(zk_ctx* ctx, int mode, int group);
 /* Streams a proof spreads its MSMs over (1..5; 0 = the default 5, or the
  * ZYKLOP_PROVE_STREAMS environment variable).  With 1 the MSMs run back to

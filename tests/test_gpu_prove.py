@@ -557,3 +557,36 @@ def test_c_and_h_msms_share_a_reduction_only_with_equal_windows(api, oracle, fil
         c.close()
     finally:
         check(L.zk_ctx_destroy(ctx))
+
+
+def test_fused_groups_replay_captured_graphs(api, oracle, files):
+    """With graphs on, each fused group's device pipeline is captured the
+    first time and replayed when the same group comes again: every replay
+    gives the single-proof results, also after another group composition
+    was captured in between, and blinded groups stay exact."""
+    circ = {nm: api.Circuit(files[nm][0]) for nm in ("u10", "c10", "u16")}
+    circ["u10"].precompute(10, 9)
+    circ["c10"].precompute(10, 9)
+    circ["u16"].precompute(12, 11)
+    wits = {nm: api.read_wtns(files[nm][1]) for nm in circ}
+    single = {nm: circ[nm].prove(wits[nm]) for nm in circ}
+    a = ["u10", "c10", "u16", "c10", "u10"]
+    b = ["u16", "u16", "c10"]
+    try:
+        api.set_batch_mode(api.BATCH_FUSED, 16)
+        api.set_graphs(True)
+        for names in (a, a, b, a, b):
+            proofs = api.prove_batch([circ[nm] for nm in names], [wits[nm] for nm in names])
+            for k, nm in enumerate(names):
+                assert np.array_equal(proofs[k], single[nm]), (names, k, nm)
+        rs, ss = [3, 5, 7], [11, 13, 17]
+        for _ in range(2):
+            bp = api.prove_batch([circ[nm] for nm in b], [wits[nm] for nm in b], rs=rs, ss=ss)
+            for k, nm in enumerate(b):
+                z, w = files[nm]
+                assert np.array_equal(bp[k], oracle.prove(blob(z), blob(w), r=rs[k], s=ss[k]))
+    finally:
+        api.set_graphs(False)
+        api.set_batch_mode(api.BATCH_AUTO, 16)
+    for c in circ.values():
+        c.close()

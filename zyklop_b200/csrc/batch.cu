@@ -68,6 +68,11 @@ void fused_init(FusedWs& f) {
   f.ready = true;
 }
 
+template <class WeOf, class PolyOf>
+void fused_pipeline(zk_ctx* ctx, FusedWs& f, Group& g, bool blind, int c1, int c2,
+                    const MsmConfig& cfgw, const MsmConfig& cfgh, const MsmConfig& cfg2,
+                    WeOf we_of, PolyOf poly_of);
+
 // Enqueues one group on f (whose previous group has been finished).  Returns
 // once host witnesses are staged; the GPU work stays in flight.
 void fused_launch(zk_ctx* ctx, FusedWs& f, Group& g, const uint64_t* const* wits, bool on_device,
@@ -130,6 +135,90 @@ void fused_launch(zk_ctx* ctx, FusedWs& f, Group& g, const uint64_t* const* wits
     else
       ctx->stager.upload(we + 4, w, 32 * (size_t)c->m1, f.s1);
   }
+  f.hsync.ensure(kHSyncWords * sizeof(uint32_t));
+  f.hflag.ensure(sizeof(uint32_t));
+  *f.hflag.as<uint32_t>() = 0;
+
+  // the device pipeline from the staged witnesses on: replayed from a graph
+  // when this group was captured before, else enqueued (and captured when
+  // graphs are on)
+  std::vector<uint64_t> key;
+  if (ctx->use_graphs) {
+    key = {(uint64_t)blind, (uint64_t)nj, (uint64_t)c1, (uint64_t)c2, (uint64_t)ctx->ntt.lmax};
+    for (const Job& j : g.jobs) {
+      key.push_back(j.c->id);
+      key.push_back((uint64_t)ctx->ntt.pass_bits[j.c->log_n]);
+    }
+    for (const MsmConfig* m : {&cfgw, &cfgh, &cfg2})
+      for (int v : {m->c, m->k0, m->k1, m->chunk}) key.push_back((uint64_t)(int64_t)v);
+    for (const void* q : {f.we.ptr, f.poly.ptr, f.g1w.ptr, f.gh.ptr, f.g2.ptr, f.win1w.ptr,
+                          f.winh.ptr, f.win2.ptr, f.hsync.ptr, f.hflag.ptr})
+      key.push_back((uint64_t)(uintptr_t)q);
+    for (FusedWs::Graph& x : f.graphs)
+      if (x.key == key) {
+        g.rw = x.rw;
+        g.rh = x.rh;
+        g.r2 = x.r2;
+        ZK_CUDA(cudaGraphLaunch(x.exec, f.s1));
+        count_launch((int)x.kernels);
+        ZK_CUDA(cudaEventRecord(f.ev_done, f.s1));
+        return;
+      }
+  }
+  Profiler* saved = current_profiler();
+  const uint64_t l0 = launch_count();
+  if (ctx->use_graphs) {
+    set_current_profiler(nullptr);  // no timing events inside a capture
+    ZK_CUDA(cudaStreamBeginCapture(f.s1, cudaStreamCaptureModeThreadLocal));
+  }
+  try {
+    fused_pipeline(ctx, f, g, blind, c1, c2, cfgw, cfgh, cfg2, we_of, poly_of);
+  } catch (...) {
+    if (ctx->use_graphs) {
+      cudaGraph_t gr = nullptr;
+      cudaStreamEndCapture(f.s1, &gr);
+      if (gr) cudaGraphDestroy(gr);
+      set_current_profiler(saved);
+    }
+    throw;
+  }
+  if (!ctx->use_graphs) {
+    ZK_CUDA(cudaEventRecord(f.ev_done, f.s1));
+    return;
+  }
+  cudaGraph_t gr = nullptr;
+  ZK_CUDA(cudaStreamEndCapture(f.s1, &gr));
+  set_current_profiler(saved);
+  FusedWs::Graph x;
+  const cudaError_t e = cudaGraphInstantiate(&x.exec, gr, 0);
+  cudaGraphDestroy(gr);
+  ZK_CUDA(e);
+  x.key = std::move(key);
+  x.rw = g.rw;
+  x.rh = g.rh;
+  x.r2 = g.r2;
+  x.kernels = launch_count() - l0;
+  if (f.graphs.size() >= FusedWs::kMaxGraphs) {
+    cudaGraphExecDestroy(f.graphs.front().exec);
+    f.graphs.erase(f.graphs.begin());
+  }
+  f.graphs.push_back(std::move(x));
+  ZK_CUDA(cudaGraphLaunch(f.graphs.back().exec, f.s1));
+  count_launch((int)f.graphs.back().kernels);
+  // recorded outside the capture: an event recorded inside one is not
+  // recorded when the graph replays
+  ZK_CUDA(cudaEventRecord(f.ev_done, f.s1));
+}
+
+// The device part of a group after its witnesses are staged on s1: it
+// begins and ends on s1 (the other streams fork from and join back to it)
+// and issues no synchronizing call, so it can be captured into a graph.
+template <class WeOf, class PolyOf>
+void fused_pipeline(zk_ctx* ctx, FusedWs& f, Group& g, bool blind, int c1, int c2,
+                    const MsmConfig& cfgw, const MsmConfig& cfgh, const MsmConfig& cfg2,
+                    WeOf we_of, PolyOf poly_of) {
+  const size_t nj = g.jobs.size();
+  const int instw = (int)nj * g.per_job, insth = (int)nj, inst2 = (int)nj;
   ZK_CUDA(cudaEventRecord(f.ev_staged, f.s1));
 
   std::vector<const void*> tab(instw);
@@ -169,39 +258,33 @@ void fused_launch(zk_ctx* ctx, FusedWs& f, Group& g, const uint64_t* const* wits
   ZK_CUDA(cudaMemcpyAsync(f.win1w.ptr, g.rw.d_data, g.rw.bytes, cudaMemcpyDeviceToHost, f.s3));
   ZK_CUDA(cudaEventRecord(f.ev_g1w, f.s3));
 
-  // SpMV per job, then one H pipeline per run of same-size jobs (one launch
-  // per stage for all of them); each size is cut into up to kPolyStreams
-  // runs so the runs overlap on the polynomial streams
-  std::map<int, std::vector<size_t>> by_size;
-  for (size_t k = 0; k < nj; k++) by_size[g.jobs[k].c->log_n].push_back(k);
-  std::vector<std::vector<size_t>> runs;
-  for (auto& kv : by_size) {
-    const size_t m = kv.second.size();
-    const size_t per = std::min<size_t>(
-        kMaxHBatch, (m + FusedWs::kPolyStreams - 1) / FusedWs::kPolyStreams);
-    for (size_t a = 0; a < m; a += per)
-      runs.emplace_back(kv.second.begin() + a, kv.second.begin() + std::min(m, a + per));
-  }
-  const int np = (int)std::min<size_t>(runs.size(), FusedWs::kPolyStreams);
+  // SpMV per job on the polynomial streams, then every job's H pipeline in
+  // one persistent launch (work items of all sizes from one device queue)
+  const int np = (int)std::min<size_t>(nj, FusedWs::kPolyStreams);
   for (int q = 0; q < np; q++) ZK_CUDA(cudaStreamWaitEvent(f.sp[q], f.ev_staged, 0));
-  for (size_t ri = 0; ri < runs.size(); ri++) {
-    cudaStream_t st = f.sp[ri % FusedWs::kPolyStreams];
-    uint64_t *aw[kMaxHBatch], *bw[kMaxHBatch], *cw[kMaxHBatch], *hh[kMaxHBatch];
-    int cnt = 0;
-    for (size_t k : runs[ri]) {
-      spmv_enqueue(g.jobs[k].c, we_of(k), poly_of(k, 0), poly_of(k, 1), st);
-      aw[cnt] = poly_of(k, 0);
-      bw[cnt] = poly_of(k, 1);
-      cw[cnt] = poly_of(k, 2);
-      hh[cnt] = poly_of(k, 3);
-      cnt++;
-    }
-    hpoly_batch(ctx->ntt, cnt, aw, bw, cw, g.jobs[runs[ri][0]].c->log_n, hh, st);
-  }
-  for (int q = 0; q < np; q++) {
+  for (size_t k = 0; k < nj; k++)
+    spmv_enqueue(g.jobs[k].c, we_of(k), poly_of(k, 0), poly_of(k, 1),
+                 f.sp[k % FusedWs::kPolyStreams]);
+  for (int q = 1; q < np; q++) {
     ZK_CUDA(cudaEventRecord(f.ev_sp[q], f.sp[q]));
-    ZK_CUDA(cudaStreamWaitEvent(f.s1, f.ev_sp[q], 0));
+    ZK_CUDA(cudaStreamWaitEvent(f.sp[0], f.ev_sp[q], 0));
   }
+  for (size_t k0 = 0; k0 < nj; k0 += kMaxHJobs) {
+    HJob hj[kMaxHJobs];
+    const size_t cnt = std::min<size_t>(kMaxHJobs, nj - k0);
+    for (size_t q = 0; q < cnt; q++) {
+      const size_t k = k0 + q;
+      hj[q] = HJob{poly_of(k, 0), poly_of(k, 1), poly_of(k, 2), poly_of(k, 3),
+                   g.jobs[k].c->log_n};
+    }
+    if (k0) ZK_CUDA(cudaMemcpyAsync(f.hflag.ptr, f.hsync.ptr, sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, f.sp[0]));  // keep an earlier timeout
+    hpoly_multi(ctx->ntt, (int)cnt, hj, f.hsync.as<uint32_t>(), f.sp[0]);
+  }
+  ZK_CUDA(cudaMemcpyAsync(f.hflag.ptr, f.hsync.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                          f.sp[0]));
+  ZK_CUDA(cudaEventRecord(f.ev_sp[0], f.sp[0]));
+  ZK_CUDA(cudaStreamWaitEvent(f.s1, f.ev_sp[0], 0));
 
   // H of every job on s1
   for (size_t k = 0; k < nj; k++) {
@@ -214,12 +297,13 @@ void fused_launch(zk_ctx* ctx, FusedWs& f, Group& g, const uint64_t* const* wits
   ZK_CUDA(cudaMemcpyAsync(f.winh.ptr, g.rh.d_data, g.rh.bytes, cudaMemcpyDeviceToHost, f.s1));
   ZK_CUDA(cudaStreamWaitEvent(f.s1, f.ev_g2, 0));
   ZK_CUDA(cudaStreamWaitEvent(f.s1, f.ev_g1w, 0));
-  ZK_CUDA(cudaEventRecord(f.ev_done, f.s1));
 }
 
 void fused_finish(FusedWs& f, const Group& g, bool blind, const uint64_t* rs, const uint64_t* ss,
                   uint64_t* proofs) {
   ZK_CUDA(cudaEventSynchronize(f.ev_done));
+  ZK_REQUIRE(!f.hflag.ptr || *f.hflag.as<uint32_t>() == 0, ZK_ETIMEOUT,
+             "fused batch: a wait inside the H pipeline gave up");
   const size_t nj = g.jobs.size();
   std::vector<ProofXyzz> px(nj);
   std::vector<uint64_t*> out(nj);
@@ -241,7 +325,13 @@ void fused_finish(FusedWs& f, const Group& g, bool blind, const uint64_t* rs, co
 
 }  // namespace
 
+void FusedWs::drop_graphs() {
+  for (Graph& g : graphs) cudaGraphExecDestroy(g.exec);
+  graphs.clear();
+}
+
 FusedWs::~FusedWs() {
+  drop_graphs();
   if (!ready) return;
   for (cudaStream_t st : {s1, s2, s3}) {
     cudaStreamSynchronize(st);

@@ -71,6 +71,20 @@ struct FusedWs {
   cudaEvent_t ev_sp[kPolyStreams] = {};
   DeviceBuffer we, poly, g1w, gh, g2;
   PinnedBuffer win1w, winh, win2;
+  DeviceBuffer hsync;  // work queue and step counters of the persistent H pipeline
+  PinnedBuffer hflag;  // its timeout flag, copied back per group
+  // captured device pipelines of groups (zk_ctx_set_graphs): one per group
+  // signature (jobs, settings and buffer addresses), replayed when the same
+  // group comes again; the MSM result metadata is kept with the graph
+  struct Graph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    MsmResult rw, rh, r2;
+    uint64_t kernels = 0;
+  };
+  static constexpr size_t kMaxGraphs = 8;
+  std::vector<Graph> graphs;
+  void drop_graphs();
   ~FusedWs();
 };
 

@@ -11,6 +11,7 @@
 #include "host_field.hpp"
 #include "ntt.hpp"
 #include "profile.hpp"
+#include "runtime.hpp"
 
 namespace zk {
 namespace {
@@ -109,16 +110,28 @@ __device__ __forceinline__ void butterfly(fr_t& u, fr_t& v, const fr_t& w, bool 
   }
 }
 
-template <bool DIT>
-__global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const fr_t* __restrict__ tw,
-                                                           int tw_shift, int L, int lo, int k,
-                                                           int log_g) {
-  extern __shared__ uint32_t sm[];
+// Loads of values other blocks of the same launch may have written (the
+// persistent H pipeline below) go around L1 (ld.global.cg); separate
+// launches use plain loads.
+template <bool CG>
+__device__ __forceinline__ fr_t fr_load(const fr_t* base, size_t idx) {
+  if (CG) {
+    const uint4* q = reinterpret_cast<const uint4*>(base) + 2 * idx;
+    const uint4 a = __ldcg(q), b = __ldcg(q + 1);
+    return fr_t{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
+  }
+  return fe_load<FrCfg>(base, idx);
+}
+
+// One tile of a pass (block `blk` of the launch that runs this pass over
+// the array in -> out).
+template <bool DIT, bool CG>
+__device__ __forceinline__ void pass_tile(const fr_t* in, fr_t* out, size_t blk,
+                                          const fr_t* __restrict__ tw, int tw_shift, int L, int lo,
+                                          int k, int log_g, uint32_t* sm) {
   const int tile = 1 << (k + log_g);
   const int G = 1 << log_g;
-  const fr_t* in = args.in[blockIdx.y];
-  fr_t* out = args.out[blockIdx.y];
-  const size_t gid0 = (size_t)blockIdx.x << log_g;
+  const size_t gid0 = blk << log_g;
   const size_t lomask = (size_t(1) << lo) - 1;
   for (int e = threadIdx.x; e < tile; e += blockDim.x) {
     int j, g;
@@ -131,7 +144,7 @@ __global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const 
     }
     const size_t gid = gid0 + g;
     const size_t idx = ((gid >> lo) << (lo + k)) | ((size_t)j << lo) | (gid & lomask);
-    sm_store(sm, tile, (j << log_g) | g, fe_load<FrCfg>(in, idx));
+    sm_store(sm, tile, (j << log_g) | g, fr_load<CG>(in, idx));
   }
   __syncthreads();
   for (int st = 0; st < k;) {
@@ -210,6 +223,15 @@ __global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const 
   }
 }
 
+template <bool DIT>
+__global__ void __launch_bounds__(kPassThreads) k_ntt_pass(PassArgs args, const fr_t* __restrict__ tw,
+                                                           int tw_shift, int L, int lo, int k,
+                                                           int log_g) {
+  extern __shared__ uint32_t sm[];
+  pass_tile<DIT, false>(args.in[blockIdx.y], args.out[blockIdx.y], blockIdx.x, tw, tw_shift, L, lo,
+                        k, log_g, sm);
+}
+
 __global__ void k_bitrev(const fr_t* __restrict__ in, fr_t* __restrict__ out, int L, bool scale,
                          fr_t factor) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,20 +242,24 @@ __global__ void k_bitrev(const fr_t* __restrict__ in, fr_t* __restrict__ out, in
   fe_store(out, r, x);
 }
 
-// C = A * B elementwise, per polynomial
+// C = A * B elementwise
+template <bool CG>
+__device__ __forceinline__ void pointwise_elem(const fr_t* a, const fr_t* b, fr_t* c, size_t i) {
+  fe_store(c, i, fr_load<CG>(a, i) * fr_load<CG>(b, i));
+}
+
 __global__ void k_pointwise_mul(const __grid_constant__ HArgs args, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
-  if (i < n) fe_store(args.c[j], i, fe_load<FrCfg>(args.a[j], i) * fe_load<FrCfg>(args.b[j], i));
+  if (i < n) pointwise_elem<false>(args.a[j], args.b[j], args.c[j], i);
 }
 
 // x[p] *= (1/N) omega_2n^rev(p) for coefficients held in bit-reversed order
 // (the coset shift of src/groth16.cu:914-921 with the INTT scale folded in).
-__global__ void k_coset_scale(PassArgs args, const fr_t* __restrict__ tw, int tw_shift, int L,
-                              fr_t c_even, fr_t c_odd) {
-  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >> L) return;
-  fr_t* a = args.in[blockIdx.y];
+template <bool CG>
+__device__ __forceinline__ void coset_elem(fr_t* a, size_t p, const fr_t* __restrict__ tw,
+                                           int tw_shift, int L, const fr_t& c_even,
+                                           const fr_t& c_odd) {
   const size_t e = L ? (__brevll((unsigned long long)p) >> (64 - L)) : 0;
   const size_t f = e >> 1;  // omega_2n^e = omega_2n^(e & 1) * omega_N^f
   const size_t half = L ? (size_t(1) << (L - 1)) : 1;
@@ -243,18 +269,28 @@ __global__ void k_coset_scale(PassArgs args, const fr_t* __restrict__ tw, int tw
   } else {
     t = fe_neg(fe_ldg<FrCfg>(tw, (f - half) << tw_shift));  // omega_N^(N/2) = -1
   }
-  fe_store(a, p, fe_load<FrCfg>(a, p) * t * ((e & 1) ? c_odd : c_even));
+  fe_store(a, p, fr_load<CG>(a, p) * t * ((e & 1) ? c_odd : c_even));
+}
+
+__global__ void k_coset_scale(PassArgs args, const fr_t* __restrict__ tw, int tw_shift, int L,
+                              fr_t c_even, fr_t c_odd) {
+  const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >> L) return;
+  coset_elem<false>(args.in[blockIdx.y], p, tw, tw_shift, L, c_even, c_odd);
 }
 
 // h = A*B - C, decoded to canonical (src/groth16.cu:935-948, 218-226), per
 // polynomial
+template <bool CG>
+__device__ __forceinline__ void h_elem(const fr_t* a, const fr_t* b, const fr_t* c, fr_t* h, size_t i) {
+  const fr_t v = fr_load<CG>(a, i) * fr_load<CG>(b, i) - fr_load<CG>(c, i);
+  fe_store(h, i, fe_from_mont(v));
+}
+
 __global__ void k_h_final(const __grid_constant__ HArgs args, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
-  if (i >= n) return;
-  const fr_t v = fe_load<FrCfg>(args.a[j], i) * fe_load<FrCfg>(args.b[j], i) -
-                 fe_load<FrCfg>(args.c[j], i);
-  fe_store(args.h[j], i, fe_from_mont(v));
+  if (i < n) h_elem<false>(args.a[j], args.b[j], args.c[j], args.h[j], i);
 }
 
 __global__ void k_fr_encode(const fr_t* __restrict__ in, fr_t* __restrict__ out, size_t n) {
@@ -415,6 +451,200 @@ void hpoly_batch(NttTables& tw, int count, uint64_t* const* aw, uint64_t* const*
 void hpoly(NttTables& tw, uint64_t* aw, uint64_t* bw, uint64_t* cw, int log_n, uint64_t* h,
            cudaStream_t st) {
   hpoly_batch(tw, 1, &aw, &bw, &cw, log_n, &h, st);
+}
+
+namespace {
+
+struct HJobDev {
+  fr_t *a, *b, *c, *h;
+  fr_t c_even, c_odd;  // coset factors: 1/N and omega_2N / N
+  uint32_t L, np, shift, elem_blocks;
+  uint32_t pass_blocks[kMaxHPasses];  // tiles per array of pass i (bit ranges low -> high)
+  uint8_t lo[kMaxHPasses], k[kMaxHPasses], log_g[kMaxHPasses];
+};
+
+struct HParams {
+  const fr_t* tw_fwd;
+  const fr_t* tw_inv;
+  uint32_t njobs, nsteps, total;
+  uint32_t off[kMaxHSteps * kMaxHJobs + 1];  // item prefix, step-major, then job
+  HJobDev job[kMaxHJobs];
+};
+
+// work items of job J at step s (0: A*B, 1..np: DIF passes high -> low,
+// np+1: coset, np+2..2np+1: DIT passes low -> high, 2np+2: h)
+__host__ __device__ inline uint32_t h_items(const HJobDev& J, uint32_t s) {
+  const uint32_t np = J.np;
+  if (s == 0 || s == 2 * np + 2) return J.elem_blocks;
+  if (s <= np) return 3 * J.pass_blocks[np - s];
+  if (s == np + 1) return 3 * J.elem_blocks;
+  if (s <= 2 * np + 1) return 3 * J.pass_blocks[s - np - 2];
+  return 0;
+}
+
+constexpr long kHMaxSpins = long(1) << 25;  // x ~64 ns: about two seconds
+
+__global__ void __launch_bounds__(kPassThreads) k_hpoly_persistent(const __grid_constant__ HParams p,
+                                                                   uint32_t* sync) {
+  extern __shared__ uint32_t sm[];
+  __shared__ uint32_t s_job, s_step, s_local, s_stop;
+  uint32_t* err = sync;
+  uint32_t* queue = sync + 1;
+  uint32_t* done = sync + 2;  // done[step * kMaxHJobs + job]
+  const uint32_t nq = p.nsteps * p.njobs;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint32_t t = atomicAdd(queue, 1u);
+      s_stop = t >= p.total;
+      if (t < p.total) {
+        uint32_t lo = 0, hi = nq;  // largest q with off[q] <= t
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (p.off[mid] <= t) lo = mid;
+          else hi = mid;
+        }
+        const uint32_t st = lo / p.njobs, jb = lo % p.njobs;
+        s_step = st;
+        s_job = jb;
+        s_local = t - p.off[lo];
+        if (st > 0) {
+          // items are taken in step order, so every item of the previous
+          // step was taken by a block that is running: the wait ends
+          const uint32_t need = h_items(p.job[jb], st - 1);
+          volatile uint32_t* d = done + (st - 1) * kMaxHJobs + jb;
+          long spins = 0;
+          while (*d < need) {
+            if (++spins > kHMaxSpins || *(volatile uint32_t*)err) {
+              atomicExch(err, 1u);
+              s_stop = 1;
+              break;
+            }
+            __nanosleep(64);
+          }
+          __threadfence();
+        }
+      }
+    }
+    __syncthreads();
+    if (s_stop) return;
+    const HJobDev& J = p.job[s_job];
+    const uint32_t st = s_step, local = s_local, np = J.np;
+    const size_t n = size_t(1) << J.L;
+    if (st == 0) {
+      const size_t i = (size_t)local * kPassThreads + threadIdx.x;
+      if (i < n) pointwise_elem<true>(J.a, J.b, J.c, i);
+    } else if (st <= np) {
+      const uint32_t pi = np - st, nb = J.pass_blocks[pi];
+      const uint32_t arr = local / nb;
+      fr_t* x = arr == 0 ? J.a : (arr == 1 ? J.b : J.c);
+      pass_tile<false, true>(x, x, local % nb, p.tw_inv, J.shift, J.L, J.lo[pi], J.k[pi],
+                             J.log_g[pi], sm);
+    } else if (st == np + 1) {
+      const uint32_t arr = local / J.elem_blocks;
+      fr_t* x = arr == 0 ? J.a : (arr == 1 ? J.b : J.c);
+      const size_t i = (size_t)(local % J.elem_blocks) * kPassThreads + threadIdx.x;
+      if (i < n) coset_elem<true>(x, i, p.tw_fwd, J.shift, J.L, J.c_even, J.c_odd);
+    } else if (st <= 2 * np + 1) {
+      const uint32_t pi = st - np - 2, nb = J.pass_blocks[pi];
+      const uint32_t arr = local / nb;
+      fr_t* x = arr == 0 ? J.a : (arr == 1 ? J.b : J.c);
+      pass_tile<true, true>(x, x, local % nb, p.tw_fwd, J.shift, J.L, J.lo[pi], J.k[pi],
+                            J.log_g[pi], sm);
+    } else {
+      const size_t i = (size_t)local * kPassThreads + threadIdx.x;
+      if (i < n) h_elem<true>(J.a, J.b, J.c, J.h, i);
+    }
+    __syncthreads();  // every thread's writes of this item precede its count
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(done + st * kMaxHJobs + s_job, 1u);
+    }
+  }
+}
+
+// Blocks per SM the persistent H pipeline takes at most: it runs beside the
+// MSM chains of the same group, so it leaves them room
+#ifndef ZK_HPOLY_PER_SM
+#define ZK_HPOLY_PER_SM 2
+#endif
+int hpoly_grid() {
+  static const int g = [] {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hpoly_persistent, kPassThreads,
+                                                      (size_t)8 * 4 * kTile) != cudaSuccess) {
+      (void)cudaGetLastError();
+      per_sm = 1;
+    }
+    per_sm = per_sm < 1 ? 1 : (per_sm > ZK_HPOLY_PER_SM ? ZK_HPOLY_PER_SM : per_sm);
+    return per_sm * device_sm_count();
+  }();
+  return g;
+}
+
+}  // namespace
+
+void hpoly_multi(NttTables& tw, int count, const HJob* jobs, uint32_t* sync, cudaStream_t st) {
+  ZK_REQUIRE(count >= 1 && count <= kMaxHJobs, ZK_EINVAL, "hpoly: 1..32 jobs per launch");
+  ZK_REQUIRE(sync, ZK_EINVAL, "hpoly: no synchronization words");
+  int lmax = 1;
+  for (int j = 0; j < count; j++) {
+    ZK_REQUIRE(jobs[j].log_n >= 1 && jobs[j].log_n < kMaxLogN, ZK_EINVAL, "hpoly: log_n out of range");
+    lmax = jobs[j].log_n > lmax ? jobs[j].log_n : lmax;
+  }
+  tw.ensure(lmax, st);
+  static_assert(sizeof(HParams) < 32000, "kernel parameters must fit the 32 KB limit");
+  HParams p{};
+  p.tw_fwd = tw.fwd.as<fr_t>();
+  p.tw_inv = tw.inv.as<fr_t>();
+  p.njobs = (uint32_t)count;
+  uint32_t nsteps = 0;
+  double units = 0;
+  for (int j = 0; j < count; j++) {
+    HJobDev& J = p.job[j];
+    const int L = jobs[j].log_n;
+    const size_t n = size_t(1) << L;
+    J.a = reinterpret_cast<fr_t*>(jobs[j].aw);
+    J.b = reinterpret_cast<fr_t*>(jobs[j].bw);
+    J.c = reinterpret_cast<fr_t*>(jobs[j].cw);
+    J.h = reinterpret_cast<fr_t*>(jobs[j].h);
+    J.L = (uint32_t)L;
+    J.shift = (uint32_t)(tw.lmax - L);
+    J.elem_blocks = (uint32_t)((n + kPassThreads - 1) / kPassThreads);
+    int lo[8], k[8];
+    const int np = split_passes(L, tw.pass_bits[L], lo, k);
+    ZK_REQUIRE(np <= kMaxHPasses, ZK_EINVAL, "hpoly: too many passes");
+    J.np = (uint32_t)np;
+    for (int i = 0; i < np; i++) {
+      const size_t groups = size_t(1) << (L - k[i]);
+      int log_g = 0;
+      while ((1 << (log_g + 1 + k[i])) <= kTile && (size_t(1) << (log_g + 1)) <= groups &&
+             (lo[i] == 0 || log_g + 1 <= lo[i]))
+        log_g++;
+      J.lo[i] = (uint8_t)lo[i];
+      J.k[i] = (uint8_t)k[i];
+      J.log_g[i] = (uint8_t)log_g;
+      J.pass_blocks[i] = (uint32_t)(groups >> log_g);
+    }
+    const Fr ninv = Fr::from_u64(n).inv();
+    J.c_even = to_dev(ninv);
+    J.c_odd = to_dev(ninv * host_root(L + 1));
+    nsteps = nsteps > 2u * np + 3u ? nsteps : 2u * np + 3u;
+    units += 6.0 * np * (double)n;
+  }
+  p.nsteps = nsteps;
+  uint32_t total = 0;
+  for (uint32_t st = 0; st < nsteps; st++)
+    for (int j = 0; j < count; j++) {
+      p.off[st * p.njobs + j] = total;
+      total += h_items(p.job[j], st);
+    }
+  p.off[nsteps * p.njobs] = total;
+  p.total = total;
+  ZK_CUDA(cudaMemsetAsync(sync, 0, kHSyncWords * sizeof(uint32_t), st));
+  const unsigned grid = (unsigned)(total < (uint32_t)hpoly_grid() ? total : hpoly_grid());
+  ProfScope prof(kProfNttPass, units, st);
+  k_hpoly_persistent<<<grid, kPassThreads, (size_t)8 * 4 * kTile, st>>>(p, sync);
+  ZK_LAUNCHED();
 }
 
 void fr_encode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t st) {

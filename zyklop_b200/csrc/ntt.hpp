@@ -57,6 +57,25 @@ constexpr int kMaxHBatch = 16;
 void hpoly_batch(NttTables& tw, int count, uint64_t* const* aw, uint64_t* const* bw,
                  uint64_t* const* cw, int log_n, uint64_t* const* h, cudaStream_t stream);
 
+// The H pipelines of up to kMaxHJobs jobs of any sizes in one persistent
+// launch: resident blocks take (job, step, tile) work items in step order
+// from a device work queue, and an item starts once every item of the same
+// job's previous step is done (steps: A*B, the DIF passes, the coset scale,
+// the DIT passes, h).  Each job's aw, bw are overwritten, cw is scratch and
+// h receives the canonical result, as in hpoly.  `sync` is kHSyncWords u32
+// of caller-owned device memory, cleared here on `stream`; a wait for a
+// previous step gives up after about two seconds and sets sync[0] to 1 (the
+// caller copies it back and fails the proof).
+constexpr int kMaxHJobs = 32;
+constexpr int kMaxHPasses = 7;                      // passes of >= 4 bits up to 2^28
+constexpr int kMaxHSteps = 2 * kMaxHPasses + 3;
+constexpr size_t kHSyncWords = 2 + (size_t)kMaxHJobs * kMaxHSteps;
+struct HJob {
+  uint64_t *aw, *bw, *cw, *h;
+  int log_n;
+};
+void hpoly_multi(NttTables& tw, int count, const HJob* jobs, uint32_t* sync, cudaStream_t stream);
+
 // Elementwise helpers over Montgomery / canonical Fr arrays.
 void fr_encode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t stream);
 void fr_decode(const uint64_t* in, uint64_t* out, size_t n, cudaStream_t stream);
