@@ -6,10 +6,12 @@
 //   after ev_staged, concurrently:
 //     s2: one multi-instance G2 MSM over every job's B2
 //     s3: one multi-instance G1 MSM over every job's A, C (and B1)
-//     sp[0..3]: SpMV per job and one batched H pipeline per run of
-//               same-size jobs (one launch per NTT stage for all of them)
+//     sp[0..3]: SpMV per job, then (on sp[0]) every job's H pipeline in one
+//               persistent launch (up to 32 jobs of any sizes per launch)
 //   s1: (after sp[]) one multi-instance G1 MSM over every job's H, then
 //       waits for s2 and s3
+// With graphs on, everything after the staging is captured the first time a
+// group of jobs comes and replayed when the same group comes again.
 // so a group costs three MSM launch chains instead of four or five per
 // proof, and each chain is as large as the group: the load-balanced
 // accumulation (persistent blocks pulling (instance, bucket-range) record
@@ -135,9 +137,11 @@ void fused_launch(zk_ctx* ctx, FusedWs& f, Group& g, const uint64_t* const* wits
     else
       ctx->stager.upload(we + 4, w, 32 * (size_t)c->m1, f.s1);
   }
+  // one status word per H launch (kMaxHJobs jobs each)
+  const size_t nh_launch = (nj + kMaxHJobs - 1) / kMaxHJobs;
   f.hsync.ensure(kHSyncWords * sizeof(uint32_t));
-  f.hflag.ensure(sizeof(uint32_t));
-  *f.hflag.as<uint32_t>() = 0;
+  f.hflag.ensure(nh_launch * sizeof(uint32_t));
+  for (size_t q = 0; q < nh_launch; q++) f.hflag.as<uint32_t>()[q] = 0;
 
   // the device pipeline from the staged witnesses on: replayed from a graph
   // when this group was captured before, else enqueued (and captured when
@@ -277,12 +281,11 @@ void fused_pipeline(zk_ctx* ctx, FusedWs& f, Group& g, bool blind, int c1, int c
       hj[q] = HJob{poly_of(k, 0), poly_of(k, 1), poly_of(k, 2), poly_of(k, 3),
                    g.jobs[k].c->log_n};
     }
-    if (k0) ZK_CUDA(cudaMemcpyAsync(f.hflag.ptr, f.hsync.ptr, sizeof(uint32_t),
-                                    cudaMemcpyDeviceToHost, f.sp[0]));  // keep an earlier timeout
     hpoly_multi(ctx->ntt, (int)cnt, hj, f.hsync.as<uint32_t>(), f.sp[0]);
+    // the launch's status word (the next launch clears the sync words)
+    ZK_CUDA(cudaMemcpyAsync(f.hflag.as<uint32_t>() + k0 / kMaxHJobs, f.hsync.ptr,
+                            sizeof(uint32_t), cudaMemcpyDeviceToHost, f.sp[0]));
   }
-  ZK_CUDA(cudaMemcpyAsync(f.hflag.ptr, f.hsync.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                          f.sp[0]));
   ZK_CUDA(cudaEventRecord(f.ev_sp[0], f.sp[0]));
   ZK_CUDA(cudaStreamWaitEvent(f.s1, f.ev_sp[0], 0));
 
@@ -302,9 +305,10 @@ void fused_pipeline(zk_ctx* ctx, FusedWs& f, Group& g, bool blind, int c1, int c
 void fused_finish(FusedWs& f, const Group& g, bool blind, const uint64_t* rs, const uint64_t* ss,
                   uint64_t* proofs) {
   ZK_CUDA(cudaEventSynchronize(f.ev_done));
-  ZK_REQUIRE(!f.hflag.ptr || *f.hflag.as<uint32_t>() == 0, ZK_ETIMEOUT,
-             "fused batch: a wait inside the H pipeline gave up");
   const size_t nj = g.jobs.size();
+  for (size_t q = 0; q < (nj + kMaxHJobs - 1) / kMaxHJobs; q++)
+    ZK_REQUIRE(f.hflag.as<uint32_t>()[q] == 0, ZK_ETIMEOUT,
+               "fused batch: a wait inside the H pipeline gave up");
   std::vector<ProofXyzz> px(nj);
   std::vector<uint64_t*> out(nj);
   for (size_t k = 0; k < nj; k++) {
