@@ -22,6 +22,10 @@ constexpr size_t kMaxWindowBytes = 2 * 64 * 256;
 // has its own); each can hold captured graphs of its device pipeline.
 struct ProveWs {
   static constexpr int kStreams = 5;  // 0: witness/SpMV/H/MSM_H, 1: A, 2: B2, 3: C, 4: B1
+  // ordered: stream priorities by chain (a proof that runs alone); workspaces
+  // whose proofs run beside others' keep equal priorities
+  explicit ProveWs(bool ordered = false) : ordered(ordered) {}
+  bool ordered = false;
   bool ready = false;
   int nstreams = kStreams;      // streams the current proof spreads its MSMs over
   int env_nstreams = kStreams;  // ZYKLOP_PROVE_STREAMS, else kStreams
@@ -100,7 +104,7 @@ struct zk_ctx {
   zk::MsmConfig msm_cfg[2];       // explicit settings (c != 0) or defaults
   zk::TuneTable tune;             // autotuned settings
   int scalar_dist = 0;            // distribution hint for zk_msm_g1 / g2
-  zk::ProveWs ws;
+  zk::ProveWs ws{true};  // single proofs (ordered streams)
   std::vector<std::unique_ptr<zk::ProveWs>> pool;  // in-flight batch workspaces
   zk::FusedWs fused[2];                            // fused batch groups (alternating)
   int batch_mode = 0;    // 0 auto, 1 in-flight pipelines, 2 fused groups

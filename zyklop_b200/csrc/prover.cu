@@ -127,15 +127,18 @@ void ProveWs::init() {
     const int v = atoi(e);
     if (v >= 1 && v <= kStreams) env_nstreams = v;
   }
-  // Stream priorities order block dispatch among a proof's MSM chains: the
-  // B2 (G2) MSM, the longest chain, first; then stream 0, whose H MSM starts
-  // only after the SpMV and the H pipeline; A, C and B1 fill the SMs left
-  // over.  Measured on a 2^20 proof: 22.9 ms against 23.4 ms with equal
-  // priorities (B2 alone first, or the H chain alone or first, gave less).
+  // Stream priorities order block dispatch among a proof's MSM chains when
+  // the proof runs alone: the B2 (G2) MSM, the longest chain, first; then
+  // stream 0, whose H MSM starts only after the SpMV and the H pipeline; A,
+  // C and B1 fill the SMs left over.  Measured on a 2^20 proof: 22.9 ms
+  // against 23.4 ms with equal priorities (B2 alone first, or the H chain
+  // alone or first, gave less).  Beside other proofs (in-flight batches, the
+  // server) every proof's B2 would outrank the rest of the device's work:
+  // batches ran ~10 % slower, so those workspaces keep equal priorities.
   int least = 0, greatest = 0;
   ZK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
   for (int i = 0; i < kStreams; i++) {
-    const int prio = i == 2 ? greatest : (i == 0 ? greatest / 2 : least);
+    const int prio = !ordered ? least : (i == 2 ? greatest : (i == 0 ? greatest / 2 : least));
     ZK_CUDA(cudaStreamCreateWithPriority(&st[i], cudaStreamNonBlocking, prio));
     ZK_CUDA(cudaEventCreateWithFlags(&ev_done[i], cudaEventDisableTiming));
   }
